@@ -1,0 +1,183 @@
+/*
+ * kerrray_cuda.h -- C ABI of the B200 (sm_100a) backend of KerrRay's per-ray hot path.
+ *
+ * The library (kerrray_b200/libkerrray_cuda.so) fills the "cuda" slot of KerrRay's backend
+ * registry.  Every entry point takes plain pointers and sizes; none keeps a pointer after it
+ * returns.  All functions return a status code (KRR_OK on success); krr_last_error() gives a
+ * thread-local message for the last failure on the calling thread.  Calls are thread-safe: the
+ * host-buffer entry points serialise per device.
+ *
+ * Reference interfaces replaced (file:line within joelprince2601/kerrray):
+ *   krr_integrate_batch         Backend.integrate_batch
+ *                               (src/kerrray/raytracing/backends/base.py:53-68), whose CPU forms are
+ *                               integrate_batch_numba (raytracing/backends/numba_backend.py:131-207)
+ *                               and integrate_rays_kernel (raytracing/backends/numba_kernel.py:467-474)
+ *   krr_integrate_batch_device  the same on device-resident buffers and a caller stream
+ *   krr_camera_states           initial_states (src/kerrray/raytracing/camera.py:298-381) for a
+ *                               pixel grid or for arbitrary image points (the PointCamera of
+ *                               scripts/study_edge_bisection.py:39-50)
+ *   krr_trace_images            compute_shadow (src/kerrray/raytracing/shadow.py:179-211) for many
+ *                               images in one persistent launch (camera, integration and
+ *                               classification on the device)
+ *   krr_max_attempts            max_attempts (src/kerrray/geodesics/integrators.py:151-162)
+ */
+#ifndef KERRRAY_CUDA_H
+#define KERRRAY_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KRR_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define KRR_API __attribute__((visibility("default")))
+#else
+#define KRR_API
+#endif
+
+/* Status codes. */
+enum {
+  KRR_OK = 0,
+  KRR_ERR_INVALID = 1,     /* invalid argument (the reference raises ValueError)            */
+  KRR_ERR_NO_DEVICE = 2,   /* no CUDA device / driver (the reference raises BackendUnavailable) */
+  KRR_ERR_CUDA = 3,        /* CUDA runtime error                                            */
+  KRR_ERR_TIMEOUT = 4,     /* a bounded device wait or deadline expired                     */
+  KRR_ERR_UNSUPPORTED = 5, /* option combination not supported by this build                */
+  KRR_ERR_NOT_NULL = 6     /* camera projection not null to 1e-10 (the reference raises RuntimeError) */
+};
+
+/* Arithmetic of the step loop. */
+enum {
+  KRR_PREC_REFERENCE = 0, /* reference operation order, no contraction; FP64 or the FP32 dtype */
+  KRR_PREC_FAST64 = 1,    /* FP64 with FMA contraction, sincos and reciprocals                */
+  KRR_PREC_MIXED = 2      /* FP32 stages, FP64 state accumulation, Delta and error norm       */
+};
+
+/* termination codes (photons/classification.py:60-69) */
+enum {
+  KRR_RUNNING = 0, KRR_ESCAPED = 1, KRR_CAPTURED = 2, KRR_MAX_AFFINE_PARAMETER = 3,
+  KRR_NUMERICAL_FAILURE = 4, KRR_OUT_OF_DOMAIN = 5, KRR_DISK_HIT = 6
+};
+
+/* IntegratorOptions + TerminationOptions + EventOptions (geodesics/integrators.py:71-148). */
+typedef struct krr_options {
+  int32_t method;          /* 0 = "rk45" (Dormand-Prince 5(4)), 1 = "rk4" */
+  int32_t dtype;           /* 0 = "float64", 1 = "float32" (reference precision mode) */
+  double rtol, atol;
+  double step_size;        /* initial (rk45) or fixed (rk4) step */
+  double lambda_max;
+  double h_min;
+  double h_max;            /* +inf for None */
+  int64_t max_steps;
+  double horizon_epsilon;  /* capture at r <= r_plus + horizon_epsilon */
+  double escape_radius;
+  int32_t disk_plane;      /* equatorial disk-plane event */
+  int32_t reserved;
+  double r_in, r_out;
+} krr_options;
+
+/* BatchResult (photons/trajectories.py:100-128).  Y, state must be non-null; the rest may be
+ * null when not wanted.  event_Y / event_hit are written only with disk_plane set. */
+typedef struct krr_result {
+  double* Y;                /* (N, 8) final states */
+  int64_t* state;           /* (N,) termination codes */
+  int64_t* n_steps;         /* (N,) accepted steps */
+  int64_t* n_rejected;      /* (N,) rejected attempts */
+  double* lam;              /* (N,) final affine parameter */
+  double* max_null_error;   /* (N,) */
+  double* max_energy_drift; /* (N,) */
+  double* max_lz_drift;     /* (N,) */
+  double* max_carter_drift; /* (N,) */
+  double* event_Y;          /* (N, 8) */
+  uint8_t* event_hit;       /* (N,) */
+} krr_result;
+
+/* Camera (raytracing/camera.py:99-204). */
+typedef struct krr_camera {
+  double radius;           /* observer Boyer-Lindquist radius r_o (M) */
+  double inclination_deg;  /* clamped into [1e-3, 180 - 1e-3] like the reference */
+  double phi_deg;
+  double fov;              /* half-width of the image plane (M) */
+  int64_t resolution;      /* even, >= 2 */
+} krr_camera;
+
+/* One image of a batched launch. */
+typedef struct krr_image {
+  double mass, spin;
+  krr_camera camera;
+  krr_options options;
+} krr_image;
+
+/* Launch shape of the persistent kernel (0 = library default / autotuned). */
+typedef struct krr_launch {
+  int32_t precision;         /* KRR_PREC_* */
+  int32_t block;             /* threads per block */
+  int32_t blocks_per_sm;     /* resident blocks per SM */
+  int32_t refill_threshold;  /* idle lanes of a warp before it refills from the queue */
+  int32_t plain;             /* 1: one thread per photon, no work queue (the plain kernel) */
+  int32_t reserved;
+} krr_launch;
+
+/* Counters of a batched launch. */
+typedef struct krr_stats {
+  uint64_t photons;     /* photons in the launch */
+  uint64_t retired;     /* photons written back (== photons) */
+  uint64_t attempts;    /* step attempts (accepted + rejected) */
+  uint64_t accepted;    /* accepted steps */
+  uint64_t lane_slots;  /* warp iterations x 32 */
+  uint64_t busy_slots;  /* lane slots that advanced a running photon */
+  double kernel_ms;     /* device time of the trace kernel (CUDA events on its stream) */
+} krr_stats;
+
+KRR_API const char* krr_last_error(void);
+KRR_API int krr_abi_version(void);
+KRR_API int krr_device_count(int* count);
+KRR_API int krr_max_attempts(const krr_options* options, int64_t* out);
+
+/* Integrate n initial states Y0 (n x 8, host) in spacetime (mass, spin) and write the result
+ * into host arrays.  runtime_s (nullable) receives the wall-clock seconds of the call. */
+KRR_API int krr_integrate_batch(int device, double mass, double spin, const double* Y0, int64_t n,
+                        const krr_options* options, int32_t precision, const krr_result* out,
+                        double* runtime_s);
+
+/* The same on device buffers (Y0 and every result array on `device`), enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream); returns without synchronising.  index
+ * (nullable, device) selects rows: ray i integrates Y0[index[i]] and writes row index[i]. */
+KRR_API int krr_integrate_batch_device(int device, double mass, double spin, const double* d_Y0,
+                               const int64_t* d_index, int64_t n, const krr_options* options,
+                               int32_t precision, const krr_result* d_out, void* stream);
+
+/* Initial states of a pixel grid (alpha == beta == NULL: resolution^2 rows, row-major) or of n
+ * arbitrary image points (alpha, beta host arrays of length n), written to host Y0 (rows x 8). */
+KRR_API int krr_camera_states(int device, double mass, double spin, const krr_camera* camera,
+                      const double* alpha, const double* beta, int64_t n, double* Y0);
+
+/* Trace many images in one persistent launch.  The photons of image k are its pixels, in
+ * row-major order, at global rows offset_k .. offset_k + resolution_k^2 (images in the given
+ * order, offsets the running sum).  Y0 (nullable, host, total x 8) replaces the camera as the
+ * photon source.  Results go to host arrays of total rows. */
+KRR_API int krr_trace_images(int device, const krr_image* images, int32_t n_images, const double* Y0,
+                     const krr_launch* launch, const krr_result* out, krr_stats* stats);
+
+/* Device form of krr_trace_images: d_Y0 (nullable) and d_out on `device`; `workspace` is
+ * krr_workspace_size(n_images) bytes of device memory owned by the caller; stream as above.
+ * Synchronises the stream before returning (the statistics are read back). */
+KRR_API size_t krr_workspace_size(int32_t n_images);
+KRR_API int krr_trace_images_device(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
+                            const krr_launch* launch, const krr_result* d_out, void* workspace,
+                            void* stream, krr_stats* stats);
+
+/* Measurement utility with no counterpart in the reference (which reports no GPU number):
+ * the FP64 (fp64 != 0) or FP32 FMA throughput of `device` in TFLOP/s (2 FLOP per FMA), from
+ * dependent FMA chains timed with CUDA events; the roofline denominator of the step kernels. */
+KRR_API int krr_fma_peak(int device, int fp64, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KERRRAY_CUDA_H */

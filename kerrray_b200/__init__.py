@@ -1,0 +1,38 @@
+"""kerrray_b200: KerrRay's per-ray ray-tracing hot path on NVIDIA B200 (sm_100a).
+
+A drop-in ``cuda`` backend for KerrRay's ``Backend`` protocol plus batched (many images in one
+persistent launch) entry points. The compute runs in ``libkerrray_cuda.so`` (hand-written CUDA
+C++ behind the C ABI of ``include/kerrray_cuda.h``); this package is the host side.
+"""
+
+from kerrray_b200._lib import BackendUnavailable
+from kerrray_b200.backends import (
+    BACKEND_NAMES,
+    Backend,
+    CudaBackend,
+    available_backends,
+    get_backend,
+    register_with_kerrray,
+)
+from kerrray_b200.camera import Camera, initial_states, initial_states_at
+from kerrray_b200.rays import concatenate_results, trace_rays
+from kerrray_b200.shadow import FAILURE_STATES, ShadowImage, compute_shadow, shadow_mask_int8, state_counts
+from kerrray_b200.sweep import DeviceSweep, ImageSpec, LaunchConfig, SweepResult, order_by_cost, trace_images
+from kerrray_b200.types import (
+    BatchResult,
+    EventOptions,
+    IntegratorOptions,
+    Spacetime,
+    TerminationOptions,
+    TerminationState,
+    max_attempts,
+    outer_horizon,
+)
+
+__all__ = [
+    "BACKEND_NAMES", "Backend", "BackendUnavailable", "BatchResult", "Camera", "CudaBackend", "DeviceSweep",
+    "EventOptions", "FAILURE_STATES", "ImageSpec", "IntegratorOptions", "LaunchConfig", "ShadowImage", "Spacetime",
+    "SweepResult", "TerminationOptions", "TerminationState", "available_backends", "compute_shadow",
+    "concatenate_results", "get_backend", "initial_states", "initial_states_at", "max_attempts", "order_by_cost",
+    "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
+]

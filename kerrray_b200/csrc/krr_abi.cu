@@ -1,0 +1,613 @@
+// Host side of the C ABI declared in include/kerrray_cuda.h: argument validation with the
+// reference's rules, parameter packing, per-device contexts with cached device buffers, and
+// the launches of the kernels in krr_ref.cu / krr_fast.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/kerrray_cuda.h"
+#include "krr_launch.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define KRR_CUDA(call)                                                                              \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess) return fail(KRR_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+constexpr double kInclinationEps = 1e-3;  // utils/config.py INCLINATION_EPSILON_DEG (camera.py:155)
+constexpr double kSafety = 0.9, kFactorMax = 5.0;
+
+// ------------------------------------------------------------------------------------------
+// Validation and packing (geodesics/integrators.py:98-129, numba_backend.py:87-115).
+// ------------------------------------------------------------------------------------------
+bool finite_pos(double x) { return std::isfinite(x) && x > 0.0; }
+
+int validate_options(const krr_options* o) {
+  if (!o) return fail(KRR_ERR_INVALID, "options must not be NULL");
+  if (o->method != 0 && o->method != 1) return fail(KRR_ERR_INVALID, "method must be 'rk45' (0) or 'rk4' (1), got %d", o->method);
+  if (o->dtype != 0 && o->dtype != 1) return fail(KRR_ERR_INVALID, "dtype must be float64 (0) or float32 (1), got %d", o->dtype);
+  const struct { const char* name; double v; } pos[] = {{"rtol", o->rtol}, {"atol", o->atol}, {"step_size", o->step_size},
+                                                      {"lambda_max", o->lambda_max}, {"h_min", o->h_min}};
+  for (const auto& p : pos)
+    if (!finite_pos(p.v)) return fail(KRR_ERR_INVALID, "%s must be a finite number > 0, got %g", p.name, p.v);
+  if (!(std::isinf(o->h_max) && o->h_max > 0) && !finite_pos(o->h_max))
+    return fail(KRR_ERR_INVALID, "h_max must be None or a finite number > 0, got %g", o->h_max);
+  if (o->max_steps < 1) return fail(KRR_ERR_INVALID, "max_steps must be >= 1, got %lld", (long long)o->max_steps);
+  if (!(std::isfinite(o->horizon_epsilon) && o->horizon_epsilon >= 0.0))
+    return fail(KRR_ERR_INVALID, "horizon_epsilon must be >= 0, got %g", o->horizon_epsilon);
+  if (!finite_pos(o->escape_radius)) return fail(KRR_ERR_INVALID, "escape_radius must be > 0, got %g", o->escape_radius);
+  if (o->disk_plane && !(0.0 < o->r_in && o->r_in <= o->r_out))
+    return fail(KRR_ERR_INVALID, "need 0 < r_in <= r_out, got r_in=%g, r_out=%g", o->r_in, o->r_out);
+  return KRR_OK;
+}
+
+int validate_spacetime(double mass, double spin) {
+  if (!finite_pos(mass)) return fail(KRR_ERR_INVALID, "mass must be a finite number > 0, got %g", mass);
+  if (!(std::isfinite(spin) && std::fabs(spin) < 1.0)) return fail(KRR_ERR_INVALID, "spin must satisfy abs(spin) < 1, got %g", spin);
+  return KRR_OK;
+}
+
+long long max_attempts(const krr_options* o) {  // integrators.py:151-162
+  const double h_max = std::max(o->lambda_max, o->step_size);
+  const double rej = (std::log(h_max / o->h_min) + (double)o->max_steps * std::log(kFactorMax)) / std::log(1.0 / kSafety);
+  return o->max_steps + (long long)std::ceil(rej) + 1;
+}
+
+double outer_horizon(double mass, double a) { return mass + std::sqrt(mass * mass - a * a); }  // horizons.py:33-42
+
+krr::Params make_params(double mass, double spin, const krr_options* o) {
+  krr::Params P{};
+  const double m = mass, a = spin * mass;
+  P.mass = m;
+  P.a = a;
+  P.a2 = a * a;
+  P.neg_2ma = (-2.0 * m) * a;
+  P.pos_2ma = (2.0 * m) * a;
+  P.two_m = 2.0 * m;
+  P.two_a2 = 2.0 * (a * a);
+  P.rtol = o->rtol;
+  P.atol = o->atol;
+  P.h0 = o->step_size;
+  P.h_min = o->h_min;
+  P.h_max = o->h_max;
+  P.lambda_max = o->lambda_max;
+  P.r_capture = outer_horizon(m, a) + o->horizon_epsilon;
+  P.r_escape = o->escape_radius;
+  P.r_in = o->disk_plane ? o->r_in : 0.0;
+  P.r_out = o->disk_plane ? o->r_out : 0.0;
+  P.max_steps = o->max_steps;
+  P.guard = max_attempts(o);
+  P.rk4 = o->method == 1;
+  P.disk = o->disk_plane != 0;
+  return P;
+}
+
+// Observer frame at (r_o, theta_o, phi_o): covariant metric (geometry/metric.py:147-163), ZAMO
+// tetrad (raytracing/camera.py:225-262) and contravariant metric (metric.py:166-195).
+int make_frame(double mass, double spin, const krr_camera* c, krr::Frame& F) {
+  if (!c) return fail(KRR_ERR_INVALID, "camera must not be NULL");
+  if (!finite_pos(c->radius)) return fail(KRR_ERR_INVALID, "radius must be a finite number > 0, got %g", c->radius);
+  if (!(std::isfinite(c->inclination_deg) && c->inclination_deg >= 0.0 && c->inclination_deg <= 180.0))
+    return fail(KRR_ERR_INVALID, "inclination_deg must lie in [0, 180], got %g", c->inclination_deg);
+  if (!std::isfinite(c->phi_deg)) return fail(KRR_ERR_INVALID, "phi_deg must be finite, got %g", c->phi_deg);
+  const double m = mass, a = spin * mass;
+  const double r = c->radius;
+  if (r <= outer_horizon(m, a))
+    return fail(KRR_ERR_INVALID, "camera radius %.6g must exceed the outer horizon r_plus = %.6g", r, outer_horizon(m, a));
+  const double incl = std::min(std::max(c->inclination_deg, kInclinationEps), 180.0 - kInclinationEps);
+  const double th = incl * (M_PI / 180.0);
+  F.r_o = r;
+  F.th_o = th;
+  F.ph_o = c->phi_deg * (M_PI / 180.0);
+  const double sn = std::sin(th), cs = std::cos(th);
+  const double s2 = sn * sn;
+  const double sig = r * r + (a * a) * (cs * cs);
+  const double dlt = r * r - 2.0 * m * r + a * a;
+  const double g_tt = -(1.0 - 2.0 * m * r / sig);
+  const double g_tphi = -2.0 * m * a * r * s2 / sig;
+  const double g_rr = sig / dlt;
+  const double g_thth = sig + 0.0 * dlt;
+  const double g_phph = (r * r + a * a + 2.0 * m * (a * a) * r * s2 / sig) * s2;
+  const double omega = -g_tphi / g_phph;
+  const double lapse2 = -(g_tt - (g_tphi * g_tphi) / g_phph);
+  if (!(lapse2 > 0.0)) return fail(KRR_ERR_INVALID, "lapse^2 = Sigma Delta / A is not positive: point is not outside the horizon");
+  const double lapse = std::sqrt(lapse2);
+  F.e00 = 1.0 / lapse;
+  F.e03 = omega / lapse;
+  F.e11 = 1.0 / std::sqrt(g_rr);
+  F.e22 = 1.0 / std::sqrt(g_thth);
+  F.e33 = 1.0 / std::sqrt(g_phph);
+  F.g_tt = g_tt;
+  F.g_tphi = g_tphi;
+  F.g_rr = g_rr;
+  F.g_thth = g_thth;
+  F.g_phph = g_phph;
+  const double r2a2 = r * r + a * a;
+  const double big_a = r2a2 * r2a2 - (a * a) * dlt * s2;
+  const double sd = sig * dlt;
+  F.gi_tt = -big_a / sd;
+  F.gi_tphi = -2.0 * m * a * r / sd;
+  F.gi_rr = dlt / sig;
+  F.gi_thth = 1.0 / sig + 0.0 * dlt;
+  F.gi_phph = (dlt - (a * a) * s2) / (sd * s2);
+  return KRR_OK;
+}
+
+int validate_grid(const krr_camera* c) {
+  if (!finite_pos(c->fov)) return fail(KRR_ERR_INVALID, "fov must be a finite number > 0, got %g", c->fov);
+  if (c->resolution < 2 || c->resolution % 2 != 0)
+    return fail(KRR_ERR_INVALID, "resolution must be an even integer >= 2, got %lld", (long long)c->resolution);
+  // The outermost pixel centre has the largest alpha^2 + beta^2 (camera.py:342-348).
+  const double n = (double)c->resolution;
+  const double edge = c->fov * (2.0 * (n - 1.0) + 1.0 - n) / n;
+  if ((edge * edge + edge * edge) / (c->radius * c->radius) >= 1.0)
+    return fail(KRR_ERR_INVALID, "fov = %.6g is too large for radius = %.6g (need fov < radius / sqrt(2))", c->fov, c->radius);
+  return KRR_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Per-device context: a stream, events and grow-only device buffers, behind a mutex.
+// ------------------------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+};
+
+enum BufId { B_Y0, B_Y, B_STATE, B_STEPS, B_REJ, B_LAM, B_NULL, B_E, B_LZ, B_Q, B_EVY, B_EVHIT, B_IMAGES, B_QUEUE, B_AB, B_ERR, B_COUNT };
+
+struct Context {
+  std::mutex mu;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int sm_count = 0;
+  DevBuf buf[B_COUNT];
+};
+
+std::mutex g_ctx_mu;
+std::vector<std::unique_ptr<Context>> g_ctx;
+
+int get_context(int device, Context** out) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(KRR_ERR_NO_DEVICE, "no CUDA device available (%s)", e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+  if (device < 0 || device >= count) return fail(KRR_ERR_INVALID, "device %d out of range [0, %d)", device, count);
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if ((int)g_ctx.size() < count) g_ctx.resize(count);
+  if (!g_ctx[device]) {
+    auto c = std::make_unique<Context>();
+    c->device = device;
+    KRR_CUDA(cudaSetDevice(device));
+    KRR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    KRR_CUDA(cudaEventCreate(&c->ev0));
+    KRR_CUDA(cudaEventCreate(&c->ev1));
+    KRR_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    g_ctx[device] = std::move(c);
+  }
+  *out = g_ctx[device].get();
+  return KRR_OK;
+}
+
+int sm_count_of(int device) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+  return n;
+}
+
+krr::Outputs to_outputs(const krr_result* r) {
+  krr::Outputs o{};
+  o.Y = r->Y;
+  o.state = reinterpret_cast<long long*>(r->state);
+  o.n_steps = reinterpret_cast<long long*>(r->n_steps);
+  o.n_rej = reinterpret_cast<long long*>(r->n_rejected);
+  o.lam = r->lam;
+  o.max_null = r->max_null_error;
+  o.max_e = r->max_energy_drift;
+  o.max_lz = r->max_lz_drift;
+  o.max_q = r->max_carter_drift;
+  o.event_Y = r->event_Y;
+  o.event_hit = r->event_hit;
+  return o;
+}
+
+int check_precision(int32_t precision, const krr_options* o) {
+  if (precision < KRR_PREC_REFERENCE || precision > KRR_PREC_MIXED)
+    return fail(KRR_ERR_INVALID, "precision must be 0 (reference), 1 (fast64) or 2 (mixed), got %d", precision);
+  if (precision != KRR_PREC_REFERENCE && o->dtype == 1)
+    return fail(KRR_ERR_UNSUPPORTED, "dtype float32 runs in the reference precision mode only");
+  if (precision == KRR_PREC_MIXED && o->method == 1)
+    return fail(KRR_ERR_UNSUPPORTED, "the mixed precision mode integrates with rk45 only");
+  return KRR_OK;
+}
+
+cudaError_t launch_plain(int32_t precision, const krr_options* o, const krr::PlainArgs& a, cudaStream_t s) {
+  const bool rk4 = o->method == 1;
+  const int block = 128;  // a multiple of 32 (the kernel's warp-aggregated counters assume it)
+  if (precision == KRR_PREC_REFERENCE) return krr::ref_plain(o->dtype == 1, rk4, a, block, s);
+  return krr::fast_plain(precision == KRR_PREC_MIXED, rk4, a, block, s);
+}
+
+// Allocate (in the context) a device copy of each requested result array.
+int device_results(Context* c, int64_t n, const krr_result* host, bool disk, krr_result* dev) {
+  std::memset(dev, 0, sizeof(*dev));
+  struct Item { BufId id; size_t bytes; bool want; void** slot; };
+  const size_t n8 = (size_t)n * 8 * sizeof(double), n1 = (size_t)n * sizeof(double);
+  Item items[] = {
+      {B_Y, n8, true, (void**)&dev->Y},
+      {B_STATE, n1, true, (void**)&dev->state},
+      {B_STEPS, n1, host->n_steps != nullptr, (void**)&dev->n_steps},
+      {B_REJ, n1, host->n_rejected != nullptr, (void**)&dev->n_rejected},
+      {B_LAM, n1, host->lam != nullptr, (void**)&dev->lam},
+      {B_NULL, n1, host->max_null_error != nullptr, (void**)&dev->max_null_error},
+      {B_E, n1, host->max_energy_drift != nullptr, (void**)&dev->max_energy_drift},
+      {B_LZ, n1, host->max_lz_drift != nullptr, (void**)&dev->max_lz_drift},
+      {B_Q, n1, host->max_carter_drift != nullptr, (void**)&dev->max_carter_drift},
+      {B_EVY, n8, disk && host->event_Y != nullptr, (void**)&dev->event_Y},
+      {B_EVHIT, (size_t)n, disk && host->event_hit != nullptr, (void**)&dev->event_hit},
+  };
+  for (auto& it : items) {
+    if (!it.want) continue;
+    KRR_CUDA(c->buf[it.id].ensure(std::max<size_t>(it.bytes, 16)));
+    *it.slot = c->buf[it.id].p;
+  }
+  if (dev->event_Y) KRR_CUDA(cudaMemsetAsync(dev->event_Y, 0, n8, c->stream));
+  if (dev->event_hit) KRR_CUDA(cudaMemsetAsync(dev->event_hit, 0, (size_t)n, c->stream));
+  return KRR_OK;
+}
+
+int copy_results_back(Context* c, int64_t n, const krr_result* dev, const krr_result* host) {
+  const size_t n8 = (size_t)n * 8 * sizeof(double), n1 = (size_t)n * sizeof(double);
+  struct Pair { void* dst; const void* src; size_t bytes; };
+  Pair pairs[] = {
+      {host->Y, dev->Y, n8}, {host->state, dev->state, n1}, {host->n_steps, dev->n_steps, n1},
+      {host->n_rejected, dev->n_rejected, n1}, {host->lam, dev->lam, n1},
+      {host->max_null_error, dev->max_null_error, n1}, {host->max_energy_drift, dev->max_energy_drift, n1},
+      {host->max_lz_drift, dev->max_lz_drift, n1}, {host->max_carter_drift, dev->max_carter_drift, n1},
+      {host->event_Y, dev->event_Y, n8}, {host->event_hit, dev->event_hit, (size_t)n},
+  };
+  for (auto& p : pairs)
+    if (p.dst && p.src && p.bytes) KRR_CUDA(cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyDeviceToHost, c->stream));
+  return KRR_OK;
+}
+
+// Images -> device descriptors with running offsets.
+int build_images(const krr_image* images, int32_t n_images, std::vector<krr::Image>& out, long long& total) {
+  if (!images || n_images < 1) return fail(KRR_ERR_INVALID, "need at least one image");
+  out.resize(n_images);
+  total = 0;
+  for (int k = 0; k < n_images; ++k) {
+    const krr_image& im = images[k];
+    int rc = validate_spacetime(im.mass, im.spin);
+    if (rc) return rc;
+    rc = validate_options(&im.options);
+    if (rc) return rc;
+    rc = make_frame(im.mass, im.spin, &im.camera, out[k].F);
+    if (rc) return rc;
+    rc = validate_grid(&im.camera);
+    if (rc) return rc;
+    out[k].P = make_params(im.mass, im.spin, &im.options);
+    out[k].fov = im.camera.fov;
+    out[k].res = im.camera.resolution;
+    out[k].offset = total;
+    out[k].count = im.camera.resolution * im.camera.resolution;
+    total += out[k].count;
+  }
+  // All images of one launch share the scheme and working precision (one kernel instance).
+  for (int k = 1; k < n_images; ++k)
+    if (images[k].options.method != images[0].options.method || images[k].options.dtype != images[0].options.dtype)
+      return fail(KRR_ERR_UNSUPPORTED, "all images of one launch must share method and dtype");
+  return KRR_OK;
+}
+
+struct LaunchShape {
+  int block, grid, refill;
+};
+
+LaunchShape persistent_shape(int device, int32_t precision, const krr_options* o, const krr_launch* l) {
+  LaunchShape s{};
+  s.block = (l && l->block > 0) ? l->block : 128;
+  const bool rk4 = o->method == 1;
+  int occ = precision == KRR_PREC_REFERENCE ? krr::ref_occupancy(o->dtype == 1, rk4, true, s.block)
+                                            : krr::fast_occupancy(precision == KRR_PREC_MIXED, rk4, true, s.block);
+  if (occ < 1) occ = 1;
+  int bps = (l && l->blocks_per_sm > 0) ? std::min(l->blocks_per_sm, occ) : occ;
+  s.grid = sm_count_of(device) * bps;
+  s.refill = (l && l->refill_threshold > 0) ? std::min(l->refill_threshold, 32) : 1;
+  return s;
+}
+
+int run_images(Context* c, const krr_image* images, const std::vector<krr::Image>& ims, long long total,
+               const double* d_Y0, const krr_launch* launch, const krr_result* d_out, void* d_work, cudaStream_t s,
+               krr_stats* stats) {
+  const int32_t precision = launch ? launch->precision : KRR_PREC_FAST64;
+  const krr_options* o0 = &images[0].options;
+  int rc = check_precision(precision, o0);
+  if (rc) return rc;
+  const size_t qbytes = (sizeof(krr::Queue) + 255) / 256 * 256;
+  krr::Queue* d_q = static_cast<krr::Queue*>(d_work);
+  krr::Image* d_images = reinterpret_cast<krr::Image*>(static_cast<char*>(d_work) + qbytes);
+  KRR_CUDA(cudaMemcpyAsync(d_images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemsetAsync(d_q, 0, sizeof(krr::Queue), s));
+  if (d_out->event_Y) KRR_CUDA(cudaMemsetAsync(d_out->event_Y, 0, (size_t)total * 8 * sizeof(double), s));
+  if (d_out->event_hit) KRR_CUDA(cudaMemsetAsync(d_out->event_hit, 0, (size_t)total, s));
+  const LaunchShape shape = persistent_shape(c->device, precision, o0, launch);
+  krr::PersistArgs a{};
+  a.images = d_images;
+  a.n_images = (int)ims.size();
+  a.total = total;
+  a.Y0 = d_Y0;
+  a.o = to_outputs(d_out);
+  a.q = d_q;
+  a.refill_threshold = shape.refill;
+  a.grid = shape.grid;
+  a.block = shape.block;
+  const bool rk4 = o0->method == 1;
+  const bool plain = launch && launch->plain;
+  KRR_CUDA(cudaEventRecord(c->ev0, s));
+  if (plain) {
+    krr::PlainArgs pa{};
+    pa.images = d_images;
+    pa.n_images = (int)ims.size();
+    pa.Y0 = d_Y0;
+    pa.n = total;
+    pa.o = a.o;
+    pa.q = d_q;
+    const int block = (launch->block > 0 && launch->block % 32 == 0) ? launch->block : 128;
+    if (precision == KRR_PREC_REFERENCE)
+      KRR_CUDA(krr::ref_plain(o0->dtype == 1, rk4, pa, block, s));
+    else
+      KRR_CUDA(krr::fast_plain(precision == KRR_PREC_MIXED, rk4, pa, block, s));
+  } else if (precision == KRR_PREC_REFERENCE) {
+    KRR_CUDA(krr::ref_persistent(o0->dtype == 1, rk4, a, s));
+  } else {
+    KRR_CUDA(krr::fast_persistent(precision == KRR_PREC_MIXED, rk4, a, s));
+  }
+  KRR_CUDA(cudaEventRecord(c->ev1, s));
+  krr::Queue q{};
+  KRR_CUDA(cudaMemcpyAsync(&q, d_q, sizeof(q), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.0f;
+  KRR_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  if (stats) {
+    stats->photons = (uint64_t)total;
+    stats->retired = q.retired;
+    stats->attempts = q.attempts;
+    stats->accepted = q.accepted;
+    stats->lane_slots = q.lane_iters;
+    stats->busy_slots = q.busy_iters;
+    stats->kernel_ms = ms;
+  }
+  if (q.error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
+  if (q.retired != (unsigned long long)total)
+    return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu photons retired of %lld", q.retired, total);
+  return KRR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* krr_last_error(void) { return g_last_error.c_str(); }
+
+int krr_abi_version(void) { return KRR_ABI_VERSION; }
+
+int krr_device_count(int* count) {
+  if (!count) return fail(KRR_ERR_INVALID, "count must not be NULL");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return fail(KRR_ERR_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+  }
+  *count = n;
+  return KRR_OK;
+}
+
+int krr_max_attempts(const krr_options* options, int64_t* out) {
+  int rc = validate_options(options);
+  if (rc) return rc;
+  if (!out) return fail(KRR_ERR_INVALID, "out must not be NULL");
+  *out = max_attempts(options);
+  return KRR_OK;
+}
+
+int krr_integrate_batch_device(int device, double mass, double spin, const double* d_Y0, const int64_t* d_index,
+                               int64_t n, const krr_options* options, int32_t precision, const krr_result* d_out,
+                               void* stream) {
+  int rc = validate_spacetime(mass, spin);
+  if (rc) return rc;
+  rc = validate_options(options);
+  if (rc) return rc;
+  rc = check_precision(precision, options);
+  if (rc) return rc;
+  if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0, got %lld", (long long)n);
+  if (n == 0) return KRR_OK;
+  if (!d_Y0 || !d_out || !d_out->Y || !d_out->state) return fail(KRR_ERR_INVALID, "Y0, Y and state must not be NULL");
+  KRR_CUDA(cudaSetDevice(device));
+  krr::PlainArgs a{};
+  a.P = make_params(mass, spin, options);
+  a.images = nullptr;
+  a.n_images = 0;
+  a.Y0 = d_Y0;
+  a.index = reinterpret_cast<const long long*>(d_index);
+  a.n = n;
+  a.o = to_outputs(d_out);
+  a.q = nullptr;
+  KRR_CUDA(launch_plain(precision, options, a, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
+int krr_integrate_batch(int device, double mass, double spin, const double* Y0, int64_t n, const krr_options* options,
+                        int32_t precision, const krr_result* out, double* runtime_s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  int rc = validate_spacetime(mass, spin);
+  if (rc) return rc;
+  rc = validate_options(options);
+  if (rc) return rc;
+  rc = check_precision(precision, options);
+  if (rc) return rc;
+  if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0, got %lld", (long long)n);
+  if (!out || (n > 0 && (!Y0 || !out->Y || !out->state))) return fail(KRR_ERR_INVALID, "Y0, Y and state must not be NULL");
+  for (int64_t i = 0; i < n * 8; ++i)
+    if (!std::isfinite(Y0[i])) return fail(KRR_ERR_INVALID, "Y0 must be finite");
+  Context* c = nullptr;
+  rc = get_context(device, &c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  KRR_CUDA(cudaSetDevice(device));
+  if (n > 0) {
+    KRR_CUDA(c->buf[B_Y0].ensure((size_t)n * 8 * sizeof(double)));
+    KRR_CUDA(cudaMemcpyAsync(c->buf[B_Y0].p, Y0, (size_t)n * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    krr_result dev;
+    rc = device_results(c, n, out, options->disk_plane != 0, &dev);
+    if (rc) return rc;
+    krr::PlainArgs a{};
+    a.P = make_params(mass, spin, options);
+    a.Y0 = static_cast<const double*>(c->buf[B_Y0].p);
+    a.n = n;
+    a.o = to_outputs(&dev);
+    KRR_CUDA(launch_plain(precision, options, a, c->stream));
+    rc = copy_results_back(c, n, &dev, out);
+    if (rc) return rc;
+    KRR_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (runtime_s) runtime_s[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return KRR_OK;
+}
+
+int krr_camera_states(int device, double mass, double spin, const krr_camera* camera, const double* alpha,
+                      const double* beta, int64_t n, double* Y0) {
+  int rc = validate_spacetime(mass, spin);
+  if (rc) return rc;
+  krr::Frame F{};
+  rc = make_frame(mass, spin, camera, F);
+  if (rc) return rc;
+  const bool grid = alpha == nullptr && beta == nullptr;
+  if (!grid && (!alpha || !beta)) return fail(KRR_ERR_INVALID, "alpha and beta must both be given or both be NULL");
+  long long rows = n;
+  if (grid) {
+    rc = validate_grid(camera);
+    if (rc) return rc;
+    rows = camera->resolution * camera->resolution;
+  } else {
+    if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0");
+    for (int64_t i = 0; i < n; ++i)
+      if (!((alpha[i] * alpha[i] + beta[i] * beta[i]) / (camera->radius * camera->radius) < 1.0))
+        return fail(KRR_ERR_INVALID, "image points with alpha^2 + beta^2 >= radius^2 are not directions on the observer's sky");
+  }
+  if (!Y0 && rows > 0) return fail(KRR_ERR_INVALID, "Y0 must not be NULL");
+  if (rows == 0) return KRR_OK;
+  Context* c = nullptr;
+  rc = get_context(device, &c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  KRR_CUDA(cudaSetDevice(device));
+  KRR_CUDA(c->buf[B_Y0].ensure((size_t)rows * 8 * sizeof(double)));
+  KRR_CUDA(c->buf[B_ERR].ensure(16));
+  KRR_CUDA(cudaMemsetAsync(c->buf[B_ERR].p, 0, 16, c->stream));
+  double* d_a = nullptr;
+  double* d_b = nullptr;
+  if (!grid) {
+    KRR_CUDA(c->buf[B_AB].ensure((size_t)rows * 2 * sizeof(double)));
+    d_a = static_cast<double*>(c->buf[B_AB].p);
+    d_b = d_a + rows;
+    KRR_CUDA(cudaMemcpyAsync(d_a, alpha, (size_t)rows * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    KRR_CUDA(cudaMemcpyAsync(d_b, beta, (size_t)rows * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  KRR_CUDA(krr::camera_states(F, camera->fov, camera->resolution, d_a, d_b, rows, static_cast<double*>(c->buf[B_Y0].p),
+                              static_cast<int*>(c->buf[B_ERR].p), c->stream));
+  int err = 0;
+  KRR_CUDA(cudaMemcpyAsync(&err, c->buf[B_ERR].p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  KRR_CUDA(cudaMemcpyAsync(Y0, c->buf[B_Y0].p, (size_t)rows * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  KRR_CUDA(cudaStreamSynchronize(c->stream));
+  if (err) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
+  return KRR_OK;
+}
+
+size_t krr_workspace_size(int32_t n_images) {
+  const size_t q = (sizeof(krr::Queue) + 255) / 256 * 256;
+  return q + (size_t)std::max(n_images, 0) * sizeof(krr::Image);
+}
+
+int krr_trace_images_device(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
+                            const krr_launch* launch, const krr_result* d_out, void* workspace, void* stream,
+                            krr_stats* stats) {
+  std::vector<krr::Image> ims;
+  long long total = 0;
+  int rc = build_images(images, n_images, ims, total);
+  if (rc) return rc;
+  if (!d_out || !d_out->Y || !d_out->state || !workspace) return fail(KRR_ERR_INVALID, "Y, state and workspace must not be NULL");
+  Context* c = nullptr;
+  rc = get_context(device, &c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  KRR_CUDA(cudaSetDevice(device));
+  return run_images(c, images, ims, total, d_Y0, launch, d_out, workspace, static_cast<cudaStream_t>(stream), stats);
+}
+
+int krr_trace_images(int device, const krr_image* images, int32_t n_images, const double* Y0, const krr_launch* launch,
+                     const krr_result* out, krr_stats* stats) {
+  std::vector<krr::Image> ims;
+  long long total = 0;
+  int rc = build_images(images, n_images, ims, total);
+  if (rc) return rc;
+  if (!out || !out->Y || !out->state) return fail(KRR_ERR_INVALID, "Y and state must not be NULL");
+  Context* c = nullptr;
+  rc = get_context(device, &c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  KRR_CUDA(cudaSetDevice(device));
+  const double* d_Y0 = nullptr;
+  if (Y0) {
+    for (long long i = 0; i < total * 8; ++i)
+      if (!std::isfinite(Y0[i])) return fail(KRR_ERR_INVALID, "Y0 must be finite");
+    KRR_CUDA(c->buf[B_Y0].ensure((size_t)total * 8 * sizeof(double)));
+    KRR_CUDA(cudaMemcpyAsync(c->buf[B_Y0].p, Y0, (size_t)total * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    d_Y0 = static_cast<const double*>(c->buf[B_Y0].p);
+  }
+  krr_result dev;
+  rc = device_results(c, total, out, images[0].options.disk_plane != 0, &dev);
+  if (rc) return rc;
+  KRR_CUDA(c->buf[B_QUEUE].ensure(krr_workspace_size(n_images)));
+  rc = run_images(c, images, ims, total, d_Y0, launch, &dev, c->buf[B_QUEUE].p, c->stream, stats);
+  if (rc) return rc;
+  rc = copy_results_back(c, total, &dev, out);
+  if (rc) return rc;
+  KRR_CUDA(cudaStreamSynchronize(c->stream));
+  return KRR_OK;
+}
+
+}  // extern "C"

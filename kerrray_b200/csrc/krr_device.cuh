@@ -1,0 +1,645 @@
+// Device code of the per-ray hot path: Kerr Boyer-Lindquist Hamiltonian right-hand side,
+// adaptive Dormand-Prince 5(4) step with the Hairer-Norsett-Wanner error norm and step
+// controller, termination classification and the conservation diagnostics.
+//
+// Semantics follow KerrRay's scalar ray kernel (src/kerrray/raytracing/backends/
+// numba_kernel.py:111-463): same state layout [t, r, theta, phi, p_t, p_r, p_theta, p_phi]
+// (geodesics/state.py:35), same tableau (geodesics/tableaus.py:59-91), same controller
+// constants and the same classification priority (photons/classification.py:72-130).
+//
+// One photon lives in one thread's registers.  p_t and p_phi are exact constants of the
+// motion in this formulation (their right-hand sides are identically zero, so the reference's
+// stage sums leave them bit-unchanged) and are carried as scalars; the other six components
+// are integrated.  Three arithmetic modes share the step/controller/classification code:
+//
+//   RefMode<double>  reference operation order in FP64 (compile the translation unit with
+//                    -fmad=false so that products and sums round separately as in the
+//                    reference's fastmath=False build);
+//   RefMode<float>   the reference's float32 working-precision mode (metric in FP64, cast);
+//   Fast64           FP64 with FMA contraction, sincos, three reciprocals instead of the
+//                    seventeen divisions, and a single-precision step-factor power;
+//   Mixed            FP32 stages (metric, right-hand side, stage sums, error estimate) with the
+//                    state accumulation y + h*sum(b_i k_i), Delta = r^2 - 2Mr + a^2 and the error
+//                    norm in FP64.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace krr {
+
+enum : int { RUNNING = 0, ESCAPED = 1, CAPTURED = 2, MAX_AFFINE = 3, FAILURE = 4, OUT_OF_DOMAIN = 5, DISK_HIT = 6 };
+
+// Integrated components (indices into the 6-vectors) and their positions in the 8-state.
+enum : int { CT = 0, CR = 1, CTH = 2, CPH = 3, CPR = 4, CPTH = 5, NV = 6 };
+
+// ------------------------------------------------------------------------------------------
+// Dormand-Prince 5(4) (Dormand & Prince 1980; Hairer, Norsett & Wanner 1993, Table 5.2).
+// ------------------------------------------------------------------------------------------
+namespace dp {
+constexpr double A10 = 1.0 / 5.0;
+constexpr double A20 = 3.0 / 40.0, A21 = 9.0 / 40.0;
+constexpr double A30 = 44.0 / 45.0, A31 = -56.0 / 15.0, A32 = 32.0 / 9.0;
+constexpr double A40 = 19372.0 / 6561.0, A41 = -25360.0 / 2187.0, A42 = 64448.0 / 6561.0, A43 = -212.0 / 729.0;
+constexpr double A50 = 9017.0 / 3168.0, A51 = -355.0 / 33.0, A52 = 46732.0 / 5247.0, A53 = 49.0 / 176.0,
+                 A54 = -5103.0 / 18656.0;
+constexpr double B0 = 35.0 / 384.0, B2 = 500.0 / 1113.0, B3 = 125.0 / 192.0, B4 = -2187.0 / 6784.0, B5 = 11.0 / 84.0;
+// Error weights E = b_hat - b (tableaus.py:85), evaluated in double like the reference.
+constexpr double E0 = 5179.0 / 57600.0 - 35.0 / 384.0;
+constexpr double E2 = 7571.0 / 16695.0 - 500.0 / 1113.0;
+constexpr double E3 = 393.0 / 640.0 - 125.0 / 192.0;
+constexpr double E4 = -92097.0 / 339200.0 - (-2187.0 / 6784.0);
+constexpr double E5 = 187.0 / 2100.0 - 11.0 / 84.0;
+constexpr double E6 = 1.0 / 40.0 - 0.0;
+// Classical RK4 (Hairer, Norsett & Wanner 1993, Table 1.2).
+constexpr double RK4_B0 = 1.0 / 6.0, RK4_B1 = 1.0 / 3.0, RK4_B2 = 1.0 / 3.0, RK4_B3 = 1.0 / 6.0;
+}  // namespace dp
+
+// Controller constants (tableaus.py:88-91).
+constexpr double SAFETY = 0.9, FACTOR_MIN = 0.2, FACTOR_MAX = 5.0, ERROR_EXPONENT = -1.0 / 5.0;
+// Classification tolerances (classification.py:53,56).
+constexpr double THETA_TOL = 1e-9, AXIS_SIN_TOL = 1e-12;
+constexpr double PI = 3.141592653589793;
+
+// ------------------------------------------------------------------------------------------
+// Parameters of one batch (or one image): geometry constants packed like numba_backend.py:96-97
+// plus the integrator, termination and event options.
+// ------------------------------------------------------------------------------------------
+struct Params {
+  double mass, a, a2, neg_2ma, pos_2ma, two_m, two_a2;
+  double rtol, atol, h0, h_min, h_max, lambda_max;
+  double r_capture, r_escape, r_in, r_out;
+  long long max_steps, guard;
+  int rk4;   // 0: Dormand-Prince 5(4), 1: fixed-step RK4
+  int disk;  // disk-plane event enabled
+};
+
+// Per-ray conservation references (numba_backend.py:174-178).  E and L_z are exact constants
+// of the integration here, so only Q0 and the floors are kept.
+struct Refs {
+  double q0, fq, fe2;
+};
+
+// ------------------------------------------------------------------------------------------
+// Arithmetic modes.
+// ------------------------------------------------------------------------------------------
+template <class X>
+__device__ __forceinline__ X py_max(X a, X b) { return (b > a) ? b : a; }  // Python max(a, b)
+template <class X>
+__device__ __forceinline__ X py_min(X a, X b) { return (b < a) ? b : a; }  // Python min(a, b)
+
+__device__ __forceinline__ bool finite_(double x) { return isfinite(x); }
+__device__ __forceinline__ bool finite_(float x) { return isfinite(x); }
+
+// Sine and cosine of the last right-hand-side evaluation, reused by classification and the
+// Carter constant (same function, same argument, so the same values the reference recomputes).
+struct Trig {
+  double s, c;
+};
+
+// Reference operation order (numba_kernel.py:111-197).  W is the working type; the metric is
+// always FP64 and cast to W before it meets the momenta.
+template <class W>
+struct RefMode {
+  using S = W;  // state type
+  using K = W;  // stage type
+  using N = W;  // error-norm type
+  static constexpr bool kFastFactor = false;
+
+  __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
+
+  __device__ static void metric(const Params& P, double r, double th, double g[15], Trig& tr) {
+    const double m = P.mass, a2 = P.a2;
+    const double s = sin(th);
+    const double c = cos(th);
+    tr.s = s;
+    tr.c = c;
+    const double s2 = s * s;
+    const double sin2th = sin(2.0 * th);
+    const double r2 = r * r;
+    const double sig = r2 + a2 * (c * c);
+    const double dlt = r2 - P.two_m * r + a2;
+    const double r2a2 = r2 + a2;
+    const double big_a = r2a2 * r2a2 - a2 * dlt * s2;
+    const double sd = sig * dlt;
+    g[0] = -big_a / sd;
+    g[1] = P.neg_2ma * r / sd;
+    g[2] = dlt / sig;
+    g[3] = 1.0 / sig;
+    g[4] = (dlt - a2 * s2) / (sd * s2);
+    const double sig_r = 2.0 * r;
+    const double sig_th = (-a2) * sin2th;
+    const double dlt_r = 2.0 * (r - m);
+    const double a_r = 4.0 * r * r2a2 - P.two_a2 * (r - m) * s2;
+    const double a_th = (-a2) * dlt * sin2th;
+    const double sd_r = sig_r * dlt + sig * dlt_r;
+    const double sd_th = sig_th * dlt;
+    const double sd2 = sd * sd;
+    const double sig2 = sig * sig;
+    g[5] = -(a_r * sd - big_a * sd_r) / sd2;
+    g[6] = P.neg_2ma * (sd - r * sd_r) / sd2;
+    g[7] = (dlt_r * sig - dlt * sig_r) / sig2;
+    g[8] = -sig_r / sig2;
+    g[9] = -sig_r / (sig2 * s2) + a2 * sd_r / sd2;
+    g[10] = -(a_th * sd - big_a * sd_th) / sd2;
+    g[11] = P.pos_2ma * r * sd_th / sd2;
+    g[12] = -dlt * sig_th / sig2;
+    g[13] = -sig_th / sig2;
+    g[14] = -(sig_th * s2 + sig * sin2th) / (sig2 * (s2 * s2)) + a2 * sd_th / sd2;
+  }
+
+  // f (6 integrated components) at state (r, th, pr, pth) with constants (pt, pph).
+  __device__ static void rhs(const Params& P, S r, S th, S pt, S pr, S pth, S pph, K f[NV], Trig& tr) {
+    double g64[15];
+    metric(P, (double)r, (double)th, g64, tr);
+    W g[15];
+#pragma unroll
+    for (int i = 0; i < 15; ++i) g[i] = (W)g64[i];
+    const W zero = (W)0.0, two = (W)2.0, neg_half = (W)-0.5;
+    W gphph = g[4], r_gphph = g[9], t_gphph = g[14];
+    if (pph == zero) {  // polar-axis guard, numba_kernel.py:177-180
+      gphph = zero;
+      r_gphph = zero;
+      t_gphph = zero;
+    }
+    f[CT] = g[0] * pt + g[1] * pph;
+    f[CR] = g[2] * pr;
+    f[CTH] = g[3] * pth;
+    f[CPH] = g[1] * pt + gphph * pph;
+    const W pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
+    f[CPR] = neg_half * (g[5] * pt2 + two * g[6] * ptpph + g[7] * pr2 + g[8] * pth2 + r_gphph * pph2);
+    f[CPTH] = neg_half * (g[10] * pt2 + two * g[11] * ptpph + g[12] * pr2 + g[13] * pth2 + t_gphph * pph2);
+  }
+};
+
+// FP64 with contraction, sincos and reciprocals.  Same closed forms as RefMode, rearranged.
+struct Fast64 {
+  using S = double;
+  using K = double;
+  using N = double;
+  static constexpr bool kFastFactor = true;
+
+  __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
+
+  __device__ static void rhs(const Params& P, double r, double th, double pt, double pr, double pth, double pph,
+                             double f[NV], Trig& tr) {
+    const double m = P.mass, a2 = P.a2;
+    double s, c;
+    sincos(th, &s, &c);
+    tr.s = s;
+    tr.c = c;
+    const double s2 = s * s;
+    const double sin2th = 2.0 * s * c;
+    const double r2 = r * r;
+    const double sig = fma(a2, c * c, r2);
+    const double dlt = fma(r, r - P.two_m, a2);
+    const double r2a2 = r2 + a2;
+    const double big_a = fma(r2a2, r2a2, -a2 * dlt * s2);
+    const double isig = 1.0 / sig;
+    const double idlt = 1.0 / dlt;
+    const double isd = isig * idlt;
+    const double isd2 = isd * isd;
+    const double isig2 = isig * isig;
+    const double sd = sig * dlt;
+    const double sig_r = 2.0 * r;
+    const double sig_th = -a2 * sin2th;
+    const double dlt_r = 2.0 * (r - m);
+    const double a_r = fma(4.0 * r, r2a2, -P.two_a2 * (r - m) * s2);
+    const double a_th = -a2 * dlt * sin2th;
+    const double sd_r = fma(sig_r, dlt, sig * dlt_r);
+    const double sd_th = sig_th * dlt;
+    const double g0 = -big_a * isd;
+    const double g1 = P.neg_2ma * r * isd;
+    const double g2 = dlt * isig;
+    const double g3 = isig;
+    const double g5 = fma(big_a, sd_r, -a_r * sd) * isd2;
+    const double g6 = P.neg_2ma * fma(-r, sd_r, sd) * isd2;
+    const double g7 = fma(dlt_r, sig, -dlt * sig_r) * isig2;
+    const double g8 = -sig_r * isig2;
+    const double g10 = fma(big_a, sd_th, -a_th * sd) * isd2;
+    const double g11 = P.pos_2ma * r * sd_th * isd2;
+    const double g12 = -dlt * sig_th * isig2;
+    const double g13 = -sig_th * isig2;
+    double g4 = 0.0, g9 = 0.0, g14 = 0.0;
+    if (pph != 0.0) {  // polar-axis guard
+      const double is2 = 1.0 / s2;
+      g4 = (dlt - a2 * s2) * isd * is2;
+      g9 = fma(-sig_r * isig2, is2, a2 * sd_r * isd2);
+      g14 = fma(-fma(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
+    }
+    f[CT] = fma(g0, pt, g1 * pph);
+    f[CR] = g2 * pr;
+    f[CTH] = g3 * pth;
+    f[CPH] = fma(g1, pt, g4 * pph);
+    const double pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
+    f[CPR] = -0.5 * fma(g5, pt2, fma(2.0 * g6, ptpph, fma(g7, pr2, fma(g8, pth2, g9 * pph2))));
+    f[CPTH] = -0.5 * fma(g10, pt2, fma(2.0 * g11, ptpph, fma(g12, pr2, fma(g13, pth2, g14 * pph2))));
+  }
+};
+
+// FP32 stages with FP64 state accumulation, FP64 Delta and FP64 error norm.
+struct Mixed {
+  using S = double;
+  using K = float;
+  using N = double;
+  static constexpr bool kFastFactor = true;
+
+  // The accepted state's diagnostics (Carter constant, axis test) use FP64 sine and cosine.
+  __device__ static Trig accept_trig(double th, const Trig&) {
+    Trig t;
+    sincos(th, &t.s, &t.c);
+    return t;
+  }
+
+  __device__ static void rhs(const Params& P, double r, double th, double pt_d, double pr_d, double pth_d,
+                             double pph_d, float f[NV], Trig& tr) {
+    // Delta near the horizon cancels to ~1e-6 of r^2: evaluate it in FP64 before the cast.
+    const float dlt = (float)fma(r, r - P.two_m, P.a2);
+    const float rf = (float)r, thf = (float)th;
+    const float m = (float)P.mass, a2 = (float)P.a2;
+    float s, c;
+    sincosf(thf, &s, &c);
+    tr.s = (double)s;
+    tr.c = (double)c;
+    const float pt = (float)pt_d, pr = (float)pr_d, pth = (float)pth_d, pph = (float)pph_d;
+    const float s2 = s * s;
+    const float sin2th = 2.0f * s * c;
+    const float r2 = rf * rf;
+    const float sig = fmaf(a2, c * c, r2);
+    const float r2a2 = r2 + a2;
+    const float big_a = fmaf(r2a2, r2a2, -a2 * dlt * s2);
+    const float isig = 1.0f / sig;
+    const float idlt = 1.0f / dlt;
+    const float isd = isig * idlt;
+    const float isd2 = isd * isd;
+    const float isig2 = isig * isig;
+    const float sd = sig * dlt;
+    const float sig_r = 2.0f * rf;
+    const float sig_th = -a2 * sin2th;
+    const float dlt_r = 2.0f * (rf - m);
+    const float a_r = fmaf(4.0f * rf, r2a2, -(float)P.two_a2 * (rf - m) * s2);
+    const float a_th = -a2 * dlt * sin2th;
+    const float sd_r = fmaf(sig_r, dlt, sig * dlt_r);
+    const float sd_th = sig_th * dlt;
+    const float neg_2ma = (float)P.neg_2ma, pos_2ma = (float)P.pos_2ma;
+    const float g0 = -big_a * isd;
+    const float g1 = neg_2ma * rf * isd;
+    const float g2 = dlt * isig;
+    const float g3 = isig;
+    const float g5 = fmaf(big_a, sd_r, -a_r * sd) * isd2;
+    const float g6 = neg_2ma * fmaf(-rf, sd_r, sd) * isd2;
+    const float g7 = fmaf(dlt_r, sig, -dlt * sig_r) * isig2;
+    const float g8 = -sig_r * isig2;
+    const float g10 = fmaf(big_a, sd_th, -a_th * sd) * isd2;
+    const float g11 = pos_2ma * rf * sd_th * isd2;
+    const float g12 = -dlt * sig_th * isig2;
+    const float g13 = -sig_th * isig2;
+    float g4 = 0.0f, g9 = 0.0f, g14 = 0.0f;
+    if (pph_d != 0.0) {
+      const float is2 = 1.0f / s2;
+      g4 = (dlt - a2 * s2) * isd * is2;
+      g9 = fmaf(-sig_r * isig2, is2, a2 * sd_r * isd2);
+      g14 = fmaf(-fmaf(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
+    }
+    f[CT] = fmaf(g0, pt, g1 * pph);
+    f[CR] = g2 * pr;
+    f[CTH] = g3 * pth;
+    f[CPH] = fmaf(g1, pt, g4 * pph);
+    const float pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
+    f[CPR] = -0.5f * fmaf(g5, pt2, fmaf(2.0f * g6, ptpph, fmaf(g7, pr2, fmaf(g8, pth2, g9 * pph2))));
+    f[CPTH] = -0.5f * fmaf(g10, pt2, fmaf(2.0f * g11, ptpph, fmaf(g12, pr2, fmaf(g13, pth2, g14 * pph2))));
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// The state of one ray between step attempts.
+// ------------------------------------------------------------------------------------------
+template <class M>
+struct Ray {
+  using S = typename M::S;
+  using K = typename M::K;
+  S y[NV];   // t, r, theta, phi, p_r, p_theta
+  S pt, pph; // constants of the motion
+  K f[NV];   // FSAL right-hand side at y
+  S h;       // proposed step (working type, like the reference's h)
+  double lam;
+  double m_null, m_q;
+  Refs ref;
+  Trig tr;   // sin/cos of theta at y
+  long long attempts;
+  int n_steps, n_rej;
+  int state;
+  bool rejected_before;
+};
+
+template <class M>
+__device__ __forceinline__ bool all_finite(const typename M::S y[NV], typename M::S pt, typename M::S pph,
+                                           const typename M::K f[NV]) {
+  bool ok = finite_(pt) && finite_(pph);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) ok = ok && finite_(y[i]) && finite_(f[i]);
+  return ok;
+}
+
+// Termination rules in the reference priority (numba_kernel.py:293-311).  Thresholds are
+// compared in the state type like the reference's working-dtype constants.
+template <class M>
+__device__ __forceinline__ int classify(const Params& P, const Ray<M>& ry, bool check_h) {
+  using S = typename M::S;
+  if (!all_finite<M>(ry.y, ry.pt, ry.pph, ry.f)) return FAILURE;
+  if (check_h && ry.h < (S)P.h_min) return FAILURE;
+  const S r = ry.y[CR], th = ry.y[CTH];
+  if (r < (S)0.0 || th < (S)(-THETA_TOL) || th > (S)(PI + THETA_TOL)) return OUT_OF_DOMAIN;
+  if (ry.pph != (S)0.0 && fabs((S)ry.tr.s) < (S)AXIS_SIN_TOL) return OUT_OF_DOMAIN;
+  if (r <= (S)P.r_capture) return CAPTURED;
+  if (r >= (S)P.r_escape && ry.f[CR] > (typename M::K)0.0) return ESCAPED;
+  if (ry.lam >= P.lambda_max || (long long)ry.n_steps >= P.max_steps) return MAX_AFFINE;
+  return RUNNING;
+}
+
+// |(1/2) p_mu dx^mu/dlambda| in FP64, sequential order (numba_kernel.py:315-321).
+template <class M>
+__device__ __forceinline__ double null_error(const Ray<M>& ry) {
+  double total = (double)ry.pt * (double)ry.f[CT];
+  total = total + (double)ry.y[CPR] * (double)ry.f[CR];
+  total = total + (double)ry.y[CPTH] * (double)ry.f[CTH];
+  total = total + (double)ry.pph * (double)ry.f[CPH];
+  return fabs(0.5 * total);
+}
+
+// Null Carter constant in FP64 (numba_kernel.py:325-336).
+template <class M>
+__device__ __forceinline__ double carter(const Params& P, const Ray<M>& ry) {
+  const double p_th = (double)ry.y[CPTH];
+  const double lz = (double)ry.pph;
+  const double e = -(double)ry.pt;
+  const double s = ry.tr.s, c = ry.tr.c;
+  double lz2_over_s2 = 0.0;
+  if (lz != 0.0) lz2_over_s2 = (lz * lz) / (s * s);
+  return p_th * p_th + (c * c) * (lz2_over_s2 - P.a2 * e * e);
+}
+
+// Set up a ray from its initial 8-state (numba_kernel.py:355-375).  q0 comes from the caller
+// (the same closed form evaluated at the initial state).
+template <class M>
+__device__ __forceinline__ void ray_init(const Params& P, const double y0[8], double q0, Ray<M>& ry) {
+  using S = typename M::S;
+  ry.y[CT] = (S)y0[0];
+  ry.y[CR] = (S)y0[1];
+  ry.y[CTH] = (S)y0[2];
+  ry.y[CPH] = (S)y0[3];
+  ry.pt = (S)y0[4];
+  ry.y[CPR] = (S)y0[5];
+  ry.y[CPTH] = (S)y0[6];
+  ry.pph = (S)y0[7];
+  // Drift floors (photons/constants.py:163-171): |E0| (1 if E0 == 0), E0^2 M^2.
+  double fe = fabs(y0[4]);
+  fe = (fe > 0.0) ? fe : 1.0;
+  ry.ref.q0 = q0;
+  ry.ref.fq = fe * fe * P.mass * P.mass;
+  ry.ref.fe2 = fe * fe;
+  M::rhs(P, ry.y[CR], ry.y[CTH], ry.pt, ry.y[CPR], ry.y[CPTH], ry.pph, ry.f, ry.tr);
+  ry.m_null = null_error<M>(ry) / ry.ref.fe2;
+  ry.m_q = 0.0;
+  ry.lam = 0.0;
+  S h = (S)P.h0;
+  if (!P.rk4 && (double)h > P.h_max) h = (S)P.h_max;
+  ry.h = h;
+  ry.attempts = 0;
+  ry.n_steps = 0;
+  ry.n_rej = 0;
+  ry.rejected_before = false;
+  ry.state = classify<M>(P, ry, false);
+}
+
+// Step factor min(5, max(0.2, 0.9 en^(-1/5))), 5 for en = 0, capped at 1 after a rejection
+// (numba_kernel.py:272-281).  The fast modes take the power in single precision
+// (en^(-1/5) = 2^(-log2(en)/5)); the reference modes call pow in the working type.
+template <class M>
+__device__ __forceinline__ typename M::N step_factor(typename M::N en, bool rejected_before) {
+  using N = typename M::N;
+  N factor;
+  if (en == (N)0.0) {
+    factor = (N)FACTOR_MAX;
+  } else {
+    N raw;
+    if constexpr (M::kFastFactor) {
+      raw = (N)(0.9f * exp2f(-0.2f * __log2f((float)en)));
+    } else {
+      raw = (N)SAFETY * pow(en, (N)ERROR_EXPONENT);
+    }
+    factor = py_min((N)FACTOR_MAX, py_max((N)FACTOR_MIN, raw));
+  }
+  if (rejected_before) factor = py_min(factor, (N)1.0);
+  return factor;
+}
+
+// One step attempt (numba_kernel.py:376-455): DP5(4) (or RK4) step, error norm, controller,
+// accept/reject, diagnostics and classification.  Returns with ry.state updated.
+template <class M, bool RK4>
+__device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __restrict__ event_y,
+                                        unsigned char* __restrict__ event_hit) {
+  using S = typename M::S;
+  using K = typename M::K;
+  using N = typename M::N;
+  ry.attempts += 1;
+  if (ry.attempts > P.guard) {  // defensive guard (integrators.py:151-162)
+    ry.state = FAILURE;
+    return;
+  }
+  const double remaining = P.lambda_max - ry.lam;
+  const bool last = (double)ry.h >= remaining;
+  const S h_eff = last ? (S)remaining : ry.h;
+  const K h = (K)h_eff;
+  K k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV];
+  S ys[NV], yn[NV];
+  Trig tr;
+  const K* k0 = ry.f;
+  if constexpr (!RK4) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)dp::A10 * k0[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k1, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)dp::A20 * k0[i] + (K)dp::A21 * k1[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k2, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      ys[i] = ry.y[i] + (S)(h * ((K)dp::A30 * k0[i] + (K)dp::A31 * k1[i] + (K)dp::A32 * k2[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k3, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      ys[i] = ry.y[i] +
+              (S)(h * ((K)dp::A40 * k0[i] + (K)dp::A41 * k1[i] + (K)dp::A42 * k2[i] + (K)dp::A43 * k3[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k4, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      ys[i] = ry.y[i] + (S)(h * ((K)dp::A50 * k0[i] + (K)dp::A51 * k1[i] + (K)dp::A52 * k2[i] +
+                                 (K)dp::A53 * k3[i] + (K)dp::A54 * k4[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k5, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      yn[i] = ry.y[i] + (S)(h * ((K)dp::B0 * k0[i] + (K)dp::B2 * k2[i] + (K)dp::B3 * k3[i] + (K)dp::B4 * k4[i] +
+                                 (K)dp::B5 * k5[i]));
+    M::rhs(P, yn[CR], yn[CTH], ry.pt, yn[CPR], yn[CPTH], ry.pph, k6, tr);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)0.5 * k0[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k1, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)0.5 * k1[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k2, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)1.0 * k2[i]));
+    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k3, tr);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      yn[i] = ry.y[i] + (S)(h * ((K)dp::RK4_B0 * k0[i] + (K)dp::RK4_B1 * k1[i] + (K)dp::RK4_B2 * k2[i] +
+                                 (K)dp::RK4_B3 * k3[i]));
+    M::rhs(P, yn[CR], yn[CTH], ry.pt, yn[CPR], yn[CPTH], ry.pph, k6, tr);
+  }
+  bool finite = true;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) finite = finite && finite_(yn[i]) && finite_(k6[i]);
+  bool accept = finite;
+  S h_new = ry.h;
+  if constexpr (!RK4) {
+    if (finite) {
+      // HNW scaled RMS norm, pairwise order ((q0+q1)+(q2+q3))+((q4+q5)+(q6+q7)) with the two
+      // constant components contributing exact zeros (numba_kernel.py:261-268).
+      N q[NV];
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        const K e = h * ((K)dp::E0 * k0[i] + (K)dp::E2 * k2[i] + (K)dp::E3 * k3[i] + (K)dp::E4 * k4[i] +
+                         (K)dp::E5 * k5[i] + (K)dp::E6 * k6[i]);
+        const N scale = (N)P.atol + (N)P.rtol * py_max((N)fabs(ry.y[i]), (N)fabs(yn[i]));
+        const N v = (N)e / scale;
+        q[i] = v * v;
+      }
+      // Full-state slots: 0 t, 1 r, 2 th, 3 ph, 4 p_t (0), 5 p_r, 6 p_th, 7 p_phi (0).
+      const N total = ((q[CT] + q[CR]) + (q[CTH] + q[CPH])) + (q[CPR] + q[CPTH]);
+      const N en = sqrt(total / (N)8.0);
+      if (!finite_(en)) {
+        finite = false;
+        accept = false;
+      } else {
+        accept = en <= (N)1.0;
+        const N factor = step_factor<M>(en, ry.rejected_before);
+        if (!(accept && last)) {
+          h_new = (S)((N)h_eff * factor);
+          if ((double)h_new > P.h_max) h_new = (S)P.h_max;
+        }
+      }
+    }
+  }
+  if (!finite) {
+    ry.state = FAILURE;
+    return;
+  }
+  const bool rejected = !accept;
+  if (rejected) ry.n_rej += 1;
+  ry.rejected_before = rejected;
+  ry.h = h_new;
+  if (rejected) {
+    if (h_new < (S)P.h_min) ry.state = FAILURE;
+    return;
+  }
+  S y_prev_th = ry.y[CTH];
+  S y_prev[NV];
+  if (P.disk) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) y_prev[i] = ry.y[i];
+  }
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    ry.y[i] = yn[i];
+    ry.f[i] = k6[i];
+  }
+  ry.tr = M::accept_trig((double)ry.y[CTH], tr);
+  const double lam_old = ry.lam;
+  ry.lam = last ? P.lambda_max : ry.lam + (double)h_eff;
+  ry.n_steps += 1;
+  // E and L_z drifts are identically zero (p_t, p_phi never change); Q and the null error:
+  ry.m_q = py_max(ry.m_q, fabs(carter<M>(P, ry) - ry.ref.q0) / py_max(fabs(ry.ref.q0), ry.ref.fq));
+  ry.m_null = py_max(ry.m_null, null_error<M>(ry) / ry.ref.fe2);
+  int code = classify<M>(P, ry, true);
+  if (P.disk) {  // disk-plane event, numba_kernel.py:439-454
+    const double half_pi = 0.5 * PI;
+    const double th_old = (double)y_prev_th;
+    const double th_new = (double)ry.y[CTH];
+    if ((th_old - half_pi) * (th_new - half_pi) < 0.0) {
+      const double s = (half_pi - th_old) / (th_new - th_old);
+      S ev[NV];
+#pragma unroll
+      for (int i = 0; i < NV; ++i) ev[i] = y_prev[i] + (S)(s * (double)(ry.y[i] - y_prev[i]));
+      ev[CTH] = (S)half_pi;
+      if (ev[CR] >= (S)P.r_in && ev[CR] <= (S)P.r_out) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) ry.y[i] = ev[i];
+        if (event_y) {
+          event_y[0] = (double)ev[CT];
+          event_y[1] = (double)ev[CR];
+          event_y[2] = (double)ev[CTH];
+          event_y[3] = (double)ev[CPH];
+          event_y[4] = (double)ry.pt;
+          event_y[5] = (double)ev[CPR];
+          event_y[6] = (double)ev[CPTH];
+          event_y[7] = (double)ry.pph;
+        }
+        if (event_hit) *event_hit = 1;
+        ry.lam = lam_old + s * (double)h_eff;
+        code = DISK_HIT;
+      }
+    }
+  }
+  ry.state = code;
+}
+
+// Null Carter constant of an initial 8-state with the sin^2/cos^2 form of
+// photons/constants.py:75-90 (the conservation reference Q0).
+__device__ __forceinline__ double carter_initial(const Params& P, const double y0[8]) {
+  const double th = y0[2], p_th = y0[6], lz = y0[7], e = -y0[4];
+  const double s = sin(th);
+  const double c = cos(th);
+  const double s2 = s * s;
+  double lz2_over_s2 = 0.0;
+  if (lz != 0.0) lz2_over_s2 = (lz * lz) / s2;
+  return p_th * p_th + (c * c) * (lz2_over_s2 - P.a2 * e * e);
+}
+
+// Output arrays of a batch (device pointers; any may be null except Y and state).
+struct Outputs {
+  double* Y;            // (N, 8)
+  long long* state;     // (N,)
+  long long* n_steps;   // (N,)
+  long long* n_rej;     // (N,)
+  double* lam;          // (N,)
+  double* max_null;     // (N,)
+  double* max_e;        // (N,)  identically zero (E is exact here)
+  double* max_lz;       // (N,)  identically zero (L_z is exact here)
+  double* max_q;        // (N,)
+  double* event_Y;      // (N, 8) or null
+  unsigned char* event_hit;  // (N,) or null
+};
+
+template <class M>
+__device__ __forceinline__ void ray_store(const Ray<M>& ry, const Outputs& o, long long n) {
+  double* Y = o.Y + n * 8;
+  Y[0] = (double)ry.y[CT];
+  Y[1] = (double)ry.y[CR];
+  Y[2] = (double)ry.y[CTH];
+  Y[3] = (double)ry.y[CPH];
+  Y[4] = (double)ry.pt;
+  Y[5] = (double)ry.y[CPR];
+  Y[6] = (double)ry.y[CPTH];
+  Y[7] = (double)ry.pph;
+  o.state[n] = ry.state;
+  if (o.n_steps) o.n_steps[n] = ry.n_steps;
+  if (o.n_rej) o.n_rej[n] = ry.n_rej;
+  if (o.lam) o.lam[n] = ry.lam;
+  if (o.max_null) o.max_null[n] = ry.m_null;
+  if (o.max_e) o.max_e[n] = 0.0;
+  if (o.max_lz) o.max_lz[n] = 0.0;
+  if (o.max_q) o.max_q[n] = ry.m_q;
+}
+
+}  // namespace krr

@@ -1,0 +1,236 @@
+// Kernels of the per-ray hot path, instantiated by krr_ref.cu (reference operation order,
+// compiled with -fmad=false) and krr_fast.cu (FMA contraction; FP64 and FP32/FP64 mixed).
+//
+//   k_trace_plain       one photon per thread from an initial-state array or an image's camera
+//                       (optionally through an index list: the FP64 re-trace of flagged
+//                       pixels), until termination;
+//   k_trace_persistent  a persistent grid over many images: each warp pulls photon indices
+//                       from a device work queue, builds the photon from its image descriptor
+//                       (camera at a finite observer distance) or from an initial-state array,
+//                       and refills lanes as photons terminate.
+#pragma once
+
+#include "krr_device.cuh"
+#include "krr_camera.cuh"
+
+namespace krr {
+
+// Which image a global photon index belongs to (images are contiguous ranges, offsets ascending).
+__device__ __forceinline__ int find_image(const Image* __restrict__ im, int n_images, long long g) {
+  int lo = 0, hi = n_images - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (im[mid].offset <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Scratch of a launch (device memory, zeroed before the launch).
+struct Queue {
+  unsigned long long head;        // next unclaimed global photon index
+  unsigned long long retired;     // photons written back (every photon exactly once)
+  unsigned long long attempts;    // step attempts, summed over rays
+  unsigned long long accepted;    // accepted steps, summed over rays
+  unsigned long long lane_iters;  // warp iterations x 32 (lane slots offered)
+  unsigned long long busy_iters;  // lane slots that advanced a running photon
+  int error;                      // KRR error code raised on the device, or 0
+  int pad;
+};
+
+// Initial state of global photon g: a row of Y0, or the camera pixel of its image.
+__device__ __forceinline__ void photon_source(const Image* __restrict__ images, int img,
+                                              const double* __restrict__ Y0, long long g, double y0[8],
+                                              Queue* q) {
+  if (Y0) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) y0[c] = Y0[g * 8 + c];
+  } else {
+    const Image& im = images[img];
+    if (camera_pixel_state(im, g - im.offset, y0) != 0 && q) atomicCAS(&q->error, 0, 6);
+  }
+}
+
+// One photon per thread.  Without images every ray uses P and a row of Y0; with images the
+// photon's image supplies the parameters and (when Y0 is null) the camera pixel.  index
+// (nullable) maps thread i to global photon index[i].
+template <class M, bool RK4>
+__global__ void k_trace_plain(Params P, const Image* __restrict__ images, int n_images,
+                              const double* __restrict__ Y0, const long long* __restrict__ index, long long n,
+                              Outputs o, Queue* q) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  unsigned long long n_att = 0, n_acc = 0, n_ret = 0;
+  if (i < n) {
+    const long long g = index ? index[i] : i;
+    double y0[8];
+    Ray<M> ry;
+    double* ev = o.event_Y ? o.event_Y + g * 8 : nullptr;
+    unsigned char* hit = o.event_hit ? o.event_hit + g : nullptr;
+    if (images) {
+      const int img = find_image(images, n_images, g);
+      photon_source(images, img, Y0, g, y0, q);
+      const Params& Pi = images[img].P;
+      ray_init<M>(Pi, y0, carter_initial(Pi, y0), ry);
+      while (ry.state == RUNNING) attempt<M, RK4>(Pi, ry, ev, hit);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) y0[c] = Y0[g * 8 + c];
+      ray_init<M>(P, y0, carter_initial(P, y0), ry);
+      while (ry.state == RUNNING) attempt<M, RK4>(P, ry, ev, hit);
+    }
+    ray_store<M>(ry, o, g);
+    n_att = (unsigned long long)ry.attempts;
+    n_acc = (unsigned long long)ry.n_steps;
+    n_ret = 1;
+  }
+  if (q) {  // warp-aggregated counters (blockDim is a multiple of 32)
+    constexpr unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      n_att += __shfl_down_sync(FULL, n_att, off);
+      n_acc += __shfl_down_sync(FULL, n_acc, off);
+      n_ret += __shfl_down_sync(FULL, n_ret, off);
+    }
+    if ((threadIdx.x & 31u) == 0 && n_ret) {
+      atomicAdd(&q->retired, n_ret);
+      atomicAdd(&q->attempts, n_att);
+      atomicAdd(&q->accepted, n_acc);
+    }
+  }
+}
+
+template <class M, bool RK4>
+__global__ void k_trace_persistent(const Image* __restrict__ images, int n_images, long long total,
+                                   const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q,
+                                   int refill_threshold) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  Ray<M> ry;
+  ry.state = FAILURE;
+  bool active = false;
+  bool drained = false;
+  long long g = -1;
+  int img = 0;
+  unsigned long long my_attempts = 0, my_accepted = 0, my_busy = 0, my_iters = 0;
+  while (true) {
+    const unsigned idle = __ballot_sync(FULL, !active);
+    const int n_idle = __popc(idle);
+    if (!drained && n_idle > 0 && (n_idle >= refill_threshold || n_idle == 32)) {
+      unsigned long long base = 0;
+      const int leader = __ffs(idle) - 1;
+      if ((int)lane == leader) base = atomicAdd(&q->head, (unsigned long long)n_idle);
+      base = __shfl_sync(FULL, base, leader);
+      if (base + (unsigned long long)n_idle >= (unsigned long long)total) drained = true;
+      if (!active) {
+        const unsigned long long mine = base + (unsigned long long)__popc(idle & lt_mask);
+        if (mine < (unsigned long long)total) {
+          g = (long long)mine;
+          img = find_image(images, n_images, g);
+          const Image& im = images[img];
+          double y0[8];
+          photon_source(images, img, Y0, g, y0, q);
+          ray_init<M>(im.P, y0, carter_initial(im.P, y0), ry);
+          if (ry.state == RUNNING) {
+            active = true;
+          } else {
+            ray_store<M>(ry, o, g);
+            atomicAdd(&q->retired, 1ull);
+          }
+        }
+      }
+    }
+    const unsigned busy = __ballot_sync(FULL, active);
+    if (busy == 0) {
+      if (drained) break;
+      continue;
+    }
+    my_iters += 1;
+    if (active) {
+      my_busy += 1;
+      const Image& im = images[img];
+      double* ev = o.event_Y ? o.event_Y + g * 8 : nullptr;
+      unsigned char* hit = o.event_hit ? o.event_hit + g : nullptr;
+      const int before = ry.n_steps;
+      attempt<M, RK4>(im.P, ry, ev, hit);
+      my_attempts += 1;
+      my_accepted += (unsigned long long)(ry.n_steps - before);
+      if (ry.state != RUNNING) {
+        ray_store<M>(ry, o, g);
+        active = false;
+        atomicAdd(&q->retired, 1ull);
+      }
+    }
+  }
+  // Per-warp statistics (one atomic per counter per warp).
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    my_attempts += __shfl_down_sync(FULL, my_attempts, off);
+    my_accepted += __shfl_down_sync(FULL, my_accepted, off);
+    my_busy += __shfl_down_sync(FULL, my_busy, off);
+  }
+  if (lane == 0) {
+    atomicAdd(&q->attempts, my_attempts);
+    atomicAdd(&q->accepted, my_accepted);
+    atomicAdd(&q->busy_iters, my_busy);
+    atomicAdd(&q->lane_iters, my_iters * 32ull);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Launch helpers shared by the two translation units.
+// ------------------------------------------------------------------------------------------
+struct PlainArgs {
+  Params P;
+  const Image* images;
+  int n_images;
+  const double* Y0;
+  const long long* index;
+  long long n;
+  Outputs o;
+  Queue* q;
+};
+
+struct PersistArgs {
+  const Image* images;
+  int n_images;
+  long long total;
+  const double* Y0;
+  Outputs o;
+  Queue* q;
+  int refill_threshold;
+  int grid;
+  int block;
+};
+
+template <class M, bool RK4>
+cudaError_t run_plain(const PlainArgs& a, int block, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  const long long grid = (a.n + block - 1) / block;
+  k_trace_plain<M, RK4><<<(unsigned)grid, block, 0, s>>>(a.P, a.images, a.n_images, a.Y0, a.index, a.n, a.o, a.q);
+  return cudaGetLastError();
+}
+
+template <class M, bool RK4>
+cudaError_t run_persistent(const PersistArgs& a, cudaStream_t s) {
+  if (a.total <= 0) return cudaSuccess;
+  k_trace_persistent<M, RK4><<<a.grid, a.block, 0, s>>>(a.images, a.n_images, a.total, a.Y0, a.o, a.q,
+                                                         a.refill_threshold);
+  return cudaGetLastError();
+}
+
+template <class M, bool RK4>
+int persistent_occupancy(int block) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_persistent<M, RK4>, block, 0) != cudaSuccess)
+    return 0;
+  return nb;
+}
+
+template <class M, bool RK4>
+int plain_occupancy(int block) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_plain<M, RK4>, block, 0) != cudaSuccess) return 0;
+  return nb;
+}
+
+}  // namespace krr

@@ -1,0 +1,54 @@
+// Kernels in the reference's operation order.  This translation unit is compiled with
+// -fmad=false: every product and sum is rounded separately, as in KerrRay's Numba kernel
+// (fastmath=False, src/kerrray/raytracing/backends/numba_kernel.py:466).
+#include "krr_launch.h"
+
+namespace krr {
+
+cudaError_t ref_plain(bool dtype32, bool rk4, const PlainArgs& a, int block, cudaStream_t s) {
+  if (dtype32) return rk4 ? run_plain<RefMode<float>, true>(a, block, s) : run_plain<RefMode<float>, false>(a, block, s);
+  return rk4 ? run_plain<RefMode<double>, true>(a, block, s) : run_plain<RefMode<double>, false>(a, block, s);
+}
+
+cudaError_t ref_persistent(bool dtype32, bool rk4, const PersistArgs& a, cudaStream_t s) {
+  if (dtype32)
+    return rk4 ? run_persistent<RefMode<float>, true>(a, s) : run_persistent<RefMode<float>, false>(a, s);
+  return rk4 ? run_persistent<RefMode<double>, true>(a, s) : run_persistent<RefMode<double>, false>(a, s);
+}
+
+int ref_occupancy(bool dtype32, bool rk4, bool persistent, int block) {
+  if (persistent) {
+    if (dtype32) return rk4 ? persistent_occupancy<RefMode<float>, true>(block) : persistent_occupancy<RefMode<float>, false>(block);
+    return rk4 ? persistent_occupancy<RefMode<double>, true>(block) : persistent_occupancy<RefMode<double>, false>(block);
+  }
+  if (dtype32) return rk4 ? plain_occupancy<RefMode<float>, true>(block) : plain_occupancy<RefMode<float>, false>(block);
+  return rk4 ? plain_occupancy<RefMode<double>, true>(block) : plain_occupancy<RefMode<double>, false>(block);
+}
+
+// Camera kernel: one image point per thread.
+__global__ void k_camera_states(Frame F, double fov, long long res, const double* __restrict__ alpha,
+                                const double* __restrict__ beta, long long n, double* __restrict__ Y0, int* err) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a, b;
+  if (alpha) {
+    a = alpha[i];
+    b = beta[i];
+  } else {
+    pixel_alpha_beta(fov, res, i, a, b);
+  }
+  double y0[8];
+  if (camera_state(F, a, b, y0) != 0 && err) atomicCAS(err, 0, 6);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) Y0[i * 8 + c] = y0[c];
+}
+
+cudaError_t camera_states(const Frame& F, double fov, long long res, const double* alpha, const double* beta,
+                          long long n, double* Y0, int* err, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int block = 256;
+  k_camera_states<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(F, fov, res, alpha, beta, n, Y0, err);
+  return cudaGetLastError();
+}
+
+}  // namespace krr

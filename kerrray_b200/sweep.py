@@ -1,0 +1,204 @@
+"""Many images in one persistent launch.
+
+An image is what ``compute_shadow`` (``src/kerrray/raytracing/shadow.py:179-211``) traces:
+a spacetime, a camera and the integrator/termination options. :func:`trace_images` puts any
+number of them (different spins, inclinations, resolutions and tolerances) into one device
+work queue: the persistent kernel builds each photon from its image's camera on the device,
+integrates it and writes its result row; warps refill lanes from the queue as photons
+terminate (``krr_trace_images``). Images are queued in the order given;
+:func:`order_by_cost` sorts them most-expensive-first so the tail of the launch is short.
+
+:class:`DeviceSweep` keeps the result arrays in device memory (torch tensors) and launches
+through ``krr_trace_images_device`` on the current torch stream -- the form the benchmark
+times with its inputs already resident.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import Any, Sequence
+
+import numpy as np
+
+from kerrray_b200 import _lib
+from kerrray_b200.camera import Camera
+from kerrray_b200.types import BatchResult, TerminationState
+
+__all__ = ["ImageSpec", "SweepResult", "DeviceSweep", "LaunchConfig", "order_by_cost", "trace_images"]
+
+
+@dataclass(frozen=True)
+class ImageSpec:
+    """One image of a batched launch."""
+
+    spacetime: Any
+    camera: Camera
+    integ: Any
+    term: Any
+    events: Any = None
+
+    @property
+    def n_rays(self) -> int:
+        return self.camera.n_rays
+
+    def as_struct(self) -> _lib.KrrImage:
+        return _lib.KrrImage(mass=float(self.spacetime.mass), spin=float(self.spacetime.spin),
+                             camera=self.camera.as_struct(), options=_lib.options_struct(self.integ, self.term, self.events))
+
+
+@dataclass(frozen=True)
+class LaunchConfig:
+    """Launch shape of the persistent kernel (0 = library default)."""
+
+    block: int = 0
+    blocks_per_sm: int = 0
+    refill_threshold: int = 0
+    plain: bool = False
+
+
+def order_by_cost(specs: Sequence[ImageSpec]) -> list[int]:
+    """Indices of ``specs`` most expensive first (steps grow like rtol^(-1/5); rays like res^2)."""
+    cost = [s.n_rays * (1.0 / s.integ.rtol) ** 0.2 for s in specs]
+    return sorted(range(len(specs)), key=lambda k: -cost[k])
+
+
+def _images(specs: Sequence[ImageSpec]):
+    if not specs:
+        raise ValueError("need at least one image")
+    arr = (_lib.KrrImage * len(specs))()
+    for k, s in enumerate(specs):
+        arr[k] = s.as_struct()
+    offsets = np.zeros(len(specs) + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum([s.n_rays for s in specs])
+    return arr, offsets
+
+
+def _launch(precision: str, cfg: LaunchConfig | None) -> _lib.KrrLaunch:
+    if precision not in _lib.PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}, got {precision!r}")
+    cfg = cfg or LaunchConfig()
+    return _lib.KrrLaunch(precision=_lib.PRECISIONS[precision], block=cfg.block, blocks_per_sm=cfg.blocks_per_sm,
+                          refill_threshold=cfg.refill_threshold, plain=int(cfg.plain), reserved=0)
+
+
+@dataclass
+class SweepResult:
+    """Flat per-photon results of a batched launch; image ``k`` owns rows ``offsets[k]:offsets[k+1]``."""
+
+    specs: list[ImageSpec]
+    offsets: np.ndarray
+    arrays: dict[str, np.ndarray]
+    stats: dict[str, Any]
+    runtime_s: float = 0.0
+    dtype32: bool = False
+
+    def rows(self, k: int) -> slice:
+        return slice(int(self.offsets[k]), int(self.offsets[k + 1]))
+
+    def result(self, k: int) -> BatchResult:
+        sl = self.rows(k)
+        a = self.arrays
+        Y = a["Y"][sl]
+        ev = a.get("event_Y")
+        return BatchResult(
+            Y=Y.astype(np.float32) if self.dtype32 else Y, state=a["state"][sl], n_steps=a["n_steps"][sl],
+            lam=a["lam"][sl], max_null_error=a["max_null_error"][sl], max_energy_drift=a["max_energy_drift"][sl],
+            max_lz_drift=a["max_lz_drift"][sl], max_carter_drift=a["max_carter_drift"][sl], runtime_s=self.runtime_s,
+            event_Y=None if ev is None else (ev[sl].astype(np.float32) if self.dtype32 else ev[sl]),
+            event_hit=None if a.get("event_hit") is None else a["event_hit"][sl].astype(bool),
+            n_rejected=a["n_rejected"][sl],
+        )
+
+    def state_image(self, k: int) -> np.ndarray:
+        return self.arrays["state"][self.rows(k)].reshape(self.specs[k].camera.shape)
+
+    def captured(self, k: int) -> np.ndarray:
+        return self.state_image(k) == int(TerminationState.CAPTURED)
+
+
+def _host_arrays(total: int, disk: bool) -> dict[str, np.ndarray | None]:
+    return {
+        "Y": np.empty((total, 8), np.float64), "state": np.empty(total, np.int64), "n_steps": np.empty(total, np.int64),
+        "n_rejected": np.empty(total, np.int64), "lam": np.empty(total, np.float64),
+        "max_null_error": np.empty(total, np.float64), "max_energy_drift": np.empty(total, np.float64),
+        "max_lz_drift": np.empty(total, np.float64), "max_carter_drift": np.empty(total, np.float64),
+        "event_Y": np.zeros((total, 8), np.float64) if disk else None,
+        "event_hit": np.zeros(total, np.uint8) if disk else None,
+    }
+
+
+def trace_images(specs: Sequence[ImageSpec], *, precision: str = "fast64", launch: LaunchConfig | None = None,
+                 device: int = 0, Y0: np.ndarray | None = None, out: dict[str, np.ndarray] | None = None) -> SweepResult:
+    """Trace every pixel of every image in one persistent launch; results in host arrays.
+
+    ``Y0`` (optional, ``(total, 8)``) replaces the cameras as the photon source (rows in image
+    order). ``out`` (optional) supplies preallocated host arrays (e.g. pinned memory).
+    """
+    import time
+
+    t0 = time.perf_counter()
+    specs = list(specs)
+    images, offsets = _images(specs)
+    total = int(offsets[-1])
+    disk = any(bool(getattr(s.events, "disk_plane", False)) for s in specs if s.events is not None)
+    arrays = out if out is not None else _host_arrays(total, disk)
+    y0 = None
+    if Y0 is not None:
+        y0 = np.ascontiguousarray(np.asarray(Y0, dtype=np.float64))
+        if y0.shape != (total, 8):
+            raise ValueError(f"Y0 must have shape ({total}, 8), got {y0.shape}")
+    res = _lib.result_struct(arrays)
+    stats = _lib.KrrStats()
+    lc = _launch(precision, launch)
+    rc = _lib.lib().krr_trace_images(device, images, len(specs), _lib.ptr(y0), ctypes.byref(lc), ctypes.byref(res),
+                                     ctypes.byref(stats))
+    _lib.check(rc)
+    dtype32 = any(str(getattr(s.integ, "dtype", "float64")) == "float32" for s in specs)
+    return SweepResult(specs=specs, offsets=offsets, arrays=arrays, stats=stats.as_dict(),
+                       runtime_s=time.perf_counter() - t0, dtype32=dtype32)
+
+
+class DeviceSweep:
+    """A batched launch whose results stay in device memory (torch tensors on ``cuda:device``).
+
+    Build once, then call :meth:`run` repeatedly; each run re-traces every image on the
+    current torch stream and returns the launch statistics (``kernel_ms`` measured with CUDA
+    events on that stream).
+    """
+
+    def __init__(self, specs: Sequence[ImageSpec], *, precision: str = "fast64", launch: LaunchConfig | None = None,
+                 device: int = 0, Y0=None, minimal: bool = False) -> None:
+        import torch
+
+        self.specs = list(specs)
+        self.images, self.offsets = _images(self.specs)
+        self.total = int(self.offsets[-1])
+        self.device = device
+        self.launch = _launch(precision, launch)
+        dev = torch.device("cuda", device)
+        n = self.total
+        f64, i64 = torch.float64, torch.int64
+        self.tensors = {"Y": torch.empty((n, 8), dtype=f64, device=dev), "state": torch.empty(n, dtype=i64, device=dev)}
+        if not minimal:
+            for name in ("n_steps", "n_rejected"):
+                self.tensors[name] = torch.empty(n, dtype=i64, device=dev)
+            for name in ("lam", "max_null_error", "max_energy_drift", "max_lz_drift", "max_carter_drift"):
+                self.tensors[name] = torch.empty(n, dtype=f64, device=dev)
+        self.Y0 = Y0
+        ws = int(_lib.lib().krr_workspace_size(len(self.specs)))
+        self.workspace = torch.zeros(max(ws, 256), dtype=torch.uint8, device=dev)
+        self._res = _lib.result_struct(self.tensors, device=True)
+
+    def run(self) -> dict[str, Any]:
+        import torch
+
+        stats = _lib.KrrStats()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        y0 = None if self.Y0 is None else self.Y0.data_ptr()
+        rc = _lib.lib().krr_trace_images_device(self.device, self.images, len(self.specs), y0, ctypes.byref(self.launch),
+                                                ctypes.byref(self._res), self.workspace.data_ptr(), stream,
+                                                ctypes.byref(stats))
+        _lib.check(rc)
+        return stats.as_dict()

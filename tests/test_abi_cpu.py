@@ -1,0 +1,163 @@
+"""CPU-only checks of the C ABI and the host logic (no kernel launches).
+
+The library must build for sm_100a, load, export every entry point ``include/kerrray_cuda.h``
+declares, and reject invalid arguments with the reference's exception types before touching
+a device (``geodesics/integrators.py:98-129``, ``raytracing/camera.py:131-168``,
+``raytracing/backends/numba_backend.py:78-84, 157-158``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, TRACE_FIXTURES, golden
+from kerrray_b200 import _lib
+from kerrray_b200.build import build
+import kerrray_b200 as K
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build()
+
+
+def test_library_exports_every_declared_symbol() -> None:
+    header = (ROOT / "include" / "kerrray_cuda.h").read_text()
+    declared = set(re.findall(r"KRR_API\s+[\w\s\*]+?\b(krr_\w+)\s*\(", header))
+    assert declared == set(_lib.EXPORTS)
+    lib = _lib.lib()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert lib.krr_abi_version() == 1
+
+
+def test_library_is_built_for_sm_100a() -> None:
+    data = (ROOT / "kerrray_b200" / "libkerrray_cuda.so").read_bytes()
+    assert b"sm_100a" in data
+
+
+@pytest.mark.parametrize("name", TRACE_FIXTURES)
+def test_max_attempts_matches_reference(name: str) -> None:
+    d = golden(name)
+    o = _lib.KrrOptions(method=0 if str(d["integ_method"]) == "rk45" else 1, dtype=0, rtol=float(d["integ_rtol"]),
+                        atol=float(d["integ_atol"]), step_size=float(d["integ_step_size"]),
+                        lambda_max=float(d["integ_lambda_max"]), h_min=float(d["integ_h_min"]),
+                        h_max=float(d["integ_h_max"]), max_steps=int(d["integ_max_steps"]),
+                        horizon_epsilon=1e-6, escape_radius=1000.0)
+    out = ctypes.c_int64()
+    assert _lib.lib().krr_max_attempts(ctypes.byref(o), ctypes.byref(out)) == 0
+    assert out.value == int(d["integ_max_attempts"])
+    integ = K.IntegratorOptions(method=str(d["integ_method"]), rtol=float(d["integ_rtol"]), atol=float(d["integ_atol"]),
+                                step_size=float(d["integ_step_size"]), max_steps=int(d["integ_max_steps"]),
+                                lambda_max=float(d["integ_lambda_max"]), h_min=float(d["integ_h_min"]))
+    assert K.max_attempts(integ) == int(d["integ_max_attempts"])
+
+
+def _opts(**kw) -> _lib.KrrOptions:
+    base = dict(method=0, dtype=0, rtol=1e-6, atol=1e-8, step_size=0.01, lambda_max=1e4, h_min=1e-12, h_max=math.inf,
+                max_steps=100000, horizon_epsilon=1e-6, escape_radius=1000.0, disk_plane=0, reserved=0, r_in=0, r_out=0)
+    base.update(kw)
+    return _lib.KrrOptions(**base)
+
+
+@pytest.mark.parametrize("bad", [dict(rtol=0.0), dict(atol=-1.0), dict(step_size=math.nan), dict(h_min=math.inf),
+                                 dict(h_max=0.0), dict(max_steps=0), dict(method=7), dict(dtype=3),
+                                 dict(horizon_epsilon=-1.0), dict(escape_radius=0.0),
+                                 dict(disk_plane=1, r_in=5.0, r_out=1.0)])
+def test_invalid_options_rejected_before_any_device_work(bad: dict) -> None:
+    y0 = np.ones((1, 8))
+    r = _lib.KrrResult()
+    rc = _lib.lib().krr_integrate_batch(0, 1.0, 0.5, y0.ctypes.data, 1, ctypes.byref(_opts(**bad)), 0, ctypes.byref(r), None)
+    assert rc == _lib.KRR_ERR_INVALID
+    assert _lib.last_error()
+
+
+def test_invalid_spacetime_and_nonfinite_input_rejected() -> None:
+    y0 = np.ones((2, 8))
+    out = {"Y": np.empty((2, 8)), "state": np.empty(2, np.int64)}
+    r = _lib.result_struct(out)
+    L = _lib.lib()
+    assert L.krr_integrate_batch(0, 1.0, 1.0, y0.ctypes.data, 2, ctypes.byref(_opts()), 0, ctypes.byref(r), None) == 1
+    assert L.krr_integrate_batch(0, -1.0, 0.5, y0.ctypes.data, 2, ctypes.byref(_opts()), 0, ctypes.byref(r), None) == 1
+    y0[1, 3] = np.inf
+    assert L.krr_integrate_batch(0, 1.0, 0.5, y0.ctypes.data, 2, ctypes.byref(_opts()), 0, ctypes.byref(r), None) == 1
+    assert "finite" in _lib.last_error()
+    # float32 runs in the reference precision only; mixed integrates rk45 only.
+    assert L.krr_integrate_batch(0, 1.0, 0.5, y0.ctypes.data, 0, ctypes.byref(_opts(dtype=1)), 1, ctypes.byref(r), None) == 5
+    assert L.krr_integrate_batch(0, 1.0, 0.5, y0.ctypes.data, 0, ctypes.byref(_opts(method=1)), 2, ctypes.byref(r), None) == 5
+
+
+def test_camera_validation_matches_reference() -> None:
+    with pytest.raises(ValueError):
+        K.Camera(radius=1000.0, inclination_deg=60.0, resolution=3)
+    with pytest.raises(ValueError):
+        K.Camera(radius=-1.0, inclination_deg=60.0)
+    with pytest.raises(ValueError):
+        K.Camera(radius=1000.0, inclination_deg=181.0)
+    assert K.Camera(radius=1000.0, inclination_deg=0.0).inclination_deg == 1e-3
+    d = golden("camera_states")
+    for k in range(int(d["n_cameras"])):
+        cam = K.Camera(radius=float(d[f"c{k}_camera_radius"]), inclination_deg=float(d[f"c{k}_camera_inclination_deg"]),
+                       phi_deg=float(d[f"c{k}_camera_phi_deg"]), fov=float(d[f"c{k}_camera_fov"]),
+                       resolution=int(d[f"c{k}_camera_resolution"]))
+        a, b = cam.pixel_coordinates()
+        assert np.array_equal(a, d[f"c{k}_alpha"]) and np.array_equal(b, d[f"c{k}_beta"])
+    # Grid checks happen on the host before any device work.
+    L = _lib.lib()
+    y = np.empty((4, 8))
+    inside = _lib.KrrCamera(radius=1.2, inclination_deg=60.0, phi_deg=0.0, fov=0.5, resolution=2)
+    assert L.krr_camera_states(0, 1.0, 0.9, ctypes.byref(inside), None, None, 0, y.ctypes.data) == 1
+    wide = _lib.KrrCamera(radius=10.0, inclination_deg=60.0, phi_deg=0.0, fov=20.0, resolution=2)
+    assert L.krr_camera_states(0, 1.0, 0.9, ctypes.byref(wide), None, None, 0, y.ctypes.data) == 1
+
+
+def test_options_validation_mirrors_reference() -> None:
+    with pytest.raises(ValueError):
+        K.IntegratorOptions(method="euler")
+    with pytest.raises(ValueError):
+        K.IntegratorOptions(h_max=0.0)
+    with pytest.raises(ValueError):
+        K.TerminationOptions(horizon_epsilon=-1.0)
+    with pytest.raises(ValueError):
+        K.EventOptions(r_in=5.0, r_out=1.0)
+    with pytest.raises(ValueError):
+        K.Spacetime(1.0, 1.0)
+    with pytest.raises(ValueError):
+        _lib.options_struct(K.IntegratorOptions(method="dop853"), K.TerminationOptions())
+
+
+def test_backend_unavailable_without_a_device() -> None:
+    if _lib.device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(K.BackendUnavailable):
+        K.CudaBackend()
+    with pytest.raises(K.BackendUnavailable):
+        K.get_backend("cuda")
+    assert K.available_backends()["cuda"] is False
+    with pytest.raises(ValueError):
+        K.get_backend("opencl")
+
+
+def test_shadow_npz_round_trip(tmp_path: Path) -> None:
+    d = golden("shadow64_a0.9_i60")
+    cam = K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=64)
+    res = K.BatchResult(Y=d["Y"], state=d["state"].astype(np.int64), n_steps=d["n_steps"].astype(np.int64),
+                        lam=d["lam"], max_null_error=d["max_null_error"], max_energy_drift=d["max_energy_drift"],
+                        max_lz_drift=d["max_lz_drift"], max_carter_drift=d["max_carter_drift"], runtime_s=0.1,
+                        n_rejected=d["n_rejected"].astype(np.int64))
+    from kerrray_b200.shadow import _image_from_result
+
+    img = _image_from_result(K.Spacetime(1.0, 0.9), cam, res)
+    assert img.count(K.TerminationState.CAPTURED) == 1250 and img.n_failed == 0 and img.n_other == 0
+    path = img.save(tmp_path / "s.npz")
+    back = K.ShadowImage.load(path)
+    assert np.array_equal(back.state, img.state) and np.array_equal(back.result.Y, img.result.Y)
+    assert back.camera == cam
+    mask = K.shadow_mask_int8(img.state)
+    assert mask.dtype == np.int8 and int((mask == 1).sum()) == 1250

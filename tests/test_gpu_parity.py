@@ -1,0 +1,182 @@
+"""GPU parity of the cuda backend against the reference's golden vectors and the oracle.
+
+Bars (from the path's specification): the termination codes must match pixel for pixel
+(any differing pixel is reported with its distance to the Bardeen curve); terminal states of
+escaped rays within 10 x rtol in ``max|dY| / max(1, |Y_ref|)``; captured rays end inside the
+capture radius. The reference-order FP64 kernel is held to more: step counts equal to the
+reference for nearly every ray.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import TRACE_FIXTURES, golden, golden_options
+
+pytestmark = pytest.mark.gpu
+
+K = pytest.importorskip("kerrray_b200")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _device():
+    from kerrray_b200.build import build
+
+    build()
+    if K._lib.device_count() < 1:
+        pytest.fail("no CUDA device: the gpu tests need a B200")
+
+
+def _opts_from(d):
+    o = golden_options(d)
+    integ = K.IntegratorOptions(method=o.method, rtol=o.rtol, atol=o.atol, step_size=o.step_size,
+                                max_steps=o.max_steps, lambda_max=o.lambda_max, h_min=o.h_min, dtype=o.dtype,
+                                h_max=o.h_max)
+    term = K.TerminationOptions(horizon_epsilon=o.horizon_epsilon, escape_radius=o.escape_radius)
+    events = K.EventOptions(disk_plane=True, r_in=o.r_in, r_out=o.r_out) if o.disk_plane else None
+    return integ, term, events
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a - b) / np.maximum(1.0, np.abs(b))
+
+
+def _compare(name: str, res, d, rtol_bar: float, min_same_steps: float) -> dict:
+    state_ref = d["state"].astype(np.int64)
+    assert np.array_equal(res.state, state_ref), f"{name}: termination codes differ at {np.flatnonzero(res.state != state_ref)[:20]}"
+    esc = state_ref == 1
+    if esc.any():
+        worst = float(np.max(_rel(res.Y[esc], d["Y"][esc])))
+        assert worst <= rtol_bar, f"{name}: escaped rays differ by {worst:.3e} > {rtol_bar:.1e}"
+    cap = state_ref == 2
+    if cap.any():
+        r_cap = 1.0 + np.sqrt(1.0 - float(d["spin"]) ** 2) + float(d["term_horizon_epsilon"])
+        assert np.all(res.Y[cap, 1] <= r_cap * (1 + 1e-12))
+    same = float(np.mean(res.n_steps == d["n_steps"].astype(np.int64)))
+    assert same >= min_same_steps, f"{name}: only {same:.3f} of the rays have the reference's step count"
+    return {"same_steps": same}
+
+
+@pytest.mark.parametrize("name", TRACE_FIXTURES)
+def test_reference_precision_matches_golden(name: str) -> None:
+    d = golden(name)
+    integ, term, events = _opts_from(d)
+    st = K.Spacetime(float(d["mass"]), float(d["spin"]))
+    res = K.CudaBackend(precision="reference").integrate_batch(st, d["Y0"], integ, term, events=events)
+    assert res.Y.dtype == (np.float32 if integ.dtype == "float32" else np.float64)
+    bar = 10 * integ.rtol if integ.dtype == "float64" else 1e-3
+    _compare(name, res, d, bar, 0.9)
+    if events is not None:
+        assert np.array_equal(res.event_hit, d["event_hit"])
+        assert np.max(_rel(res.event_Y, d["event_Y"])) < 1e-6
+    assert np.all(res.max_energy_drift == 0.0) and np.all(res.max_lz_drift == 0.0)
+    nz = d["max_null_error"] > 0
+    if integ.dtype == "float64" and nz.any():
+        # diagnostics: same magnitude as the reference's running maxima
+        ratio = res.max_null_error[nz] / d["max_null_error"][nz]
+        assert np.median(ratio) == pytest.approx(1.0, rel=1e-3)
+
+
+@pytest.mark.parametrize("name", ["shadow64_a0.9_i60", "camera24_rtol1e-8", "hmax_3", "schwarzschild_6x6_rtol1e-9",
+                                  "failures_512_rtol1e-4", "axis_lz0", "tangential_photons_a0"])
+def test_fast64_matches_golden(name: str) -> None:
+    d = golden(name)
+    integ, term, events = _opts_from(d)
+    st = K.Spacetime(float(d["mass"]), float(d["spin"]))
+    res = K.CudaBackend(precision="fast64").integrate_batch(st, d["Y0"], integ, term, events=events)
+    _compare(name, res, d, 10 * integ.rtol, 0.5)
+
+
+def test_camera_states_match_reference() -> None:
+    d = golden("camera_states")
+    for k in range(int(d["n_cameras"])):
+        st = K.Spacetime(float(d[f"c{k}_mass"]), float(d[f"c{k}_spin"]))
+        cam = K.Camera(radius=float(d[f"c{k}_camera_radius"]), inclination_deg=float(d[f"c{k}_camera_inclination_deg"]),
+                       phi_deg=float(d[f"c{k}_camera_phi_deg"]), fov=float(d[f"c{k}_camera_fov"]),
+                       resolution=int(d[f"c{k}_camera_resolution"]))
+        y = K.initial_states(cam, st)
+        ref = d[f"c{k}_Y0"]
+        assert np.max(_rel(y, ref)) < 1e-12, k
+        back = K.initial_states(cam, st, reverse=False)
+        assert np.array_equal(back[:, 4:], -y[:, 4:])
+        a, b = d[f"c{k}_alpha"].ravel(), d[f"c{k}_beta"].ravel()
+        pts = K.initial_states_at(st, cam.radius, cam.inclination_deg, a, b, phi_deg=cam.phi_deg)
+        assert np.array_equal(pts, y)
+
+
+def test_persistent_launch_equals_plain_kernel() -> None:
+    """The work-queue kernel runs the same per-ray code: bit-identical results and a full retire count."""
+    d = golden("shadow64_a0.9_i60")
+    st = K.Spacetime(1.0, 0.9)
+    cam = K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=64)
+    integ = K.IntegratorOptions(method="rk45", rtol=1e-6, atol=1e-8)
+    term = K.TerminationOptions()
+    spec = K.ImageSpec(st, cam, integ, term)
+    for precision in ("reference", "fast64"):
+        plain = K.CudaBackend(precision=precision).integrate_batch(st, d["Y0"], integ, term)
+        for cfg in (K.LaunchConfig(), K.LaunchConfig(block=64, refill_threshold=8), K.LaunchConfig(blocks_per_sm=1)):
+            sw = K.trace_images([spec], precision=precision, Y0=d["Y0"], launch=cfg)
+            r = sw.result(0)
+            assert np.array_equal(r.state, plain.state) and np.array_equal(r.Y, plain.Y)
+            assert np.array_equal(r.n_steps, plain.n_steps) and np.array_equal(r.n_rejected, plain.n_rejected)
+            assert sw.stats["retired"] == sw.stats["photons"] == 4096
+            assert sw.stats["attempts"] == int(r.n_steps.sum() + r.n_rejected.sum())
+            assert sw.stats["accepted"] == int(r.n_steps.sum())
+
+
+def test_shadow_image_on_device_camera_matches_reference_mask() -> None:
+    """64 x 64, a* = 0.9, i = 60 deg, +-8 M, rtol 1e-6: camera, integration and mask on the device."""
+    d = golden("shadow64_a0.9_i60")
+    bard = golden("bardeen_curves")
+    st = K.Spacetime(1.0, 0.9)
+    cam = K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=64)
+    integ = K.IntegratorOptions(method="rk45", rtol=1e-6, atol=1e-8)
+    for precision in ("reference", "fast64", "mixed"):
+        img = K.compute_shadow(st, cam, integ, K.TerminationOptions(), backend=K.CudaBackend(precision=precision))
+        diff = np.flatnonzero(img.state.ravel() != d["state"])
+        if diff.size:
+            # Report each differing pixel with its distance (px) to the Bardeen curve.
+            ca, cb = bard["curve_0.9_60_alpha"], bard["curve_0.9_60_beta"]
+            k = float(bard["kscale_0.9_1000"])
+            a, b = img.alpha.ravel()[diff] * k, img.beta.ravel()[diff] * k
+            dist = np.min(np.hypot(a[:, None] - ca[None, :], b[:, None] - cb[None, :]), axis=1) / (cam.pixel_size * k)
+            print(f"{precision}: {diff.size} differing pixels at Bardeen distance {np.round(dist, 4).tolist()} px")
+            assert diff.size <= 2 and np.all(dist < 0.05), (precision, diff.tolist(), dist.tolist())
+        assert img.count(K.TerminationState.CAPTURED) + img.count(K.TerminationState.ESCAPED) == 4096
+
+
+def test_sweep_sample_all_spins_inclinations_tolerances() -> None:
+    d = golden("sweep_sample_128")
+    be = K.CudaBackend(precision="reference")
+    same_steps = []
+    for j in range(len(d["spin"])):
+        rtol = float(d["rtol"][j])
+        st = K.Spacetime(1.0, float(d["spin"][j]))
+        res = be.integrate_batch(st, d["Y0"][j], K.IntegratorOptions(rtol=rtol, atol=1e-2 * rtol), K.TerminationOptions())
+        assert np.array_equal(res.state, d["state"][j].astype(np.int64)), j
+        esc = d["state"][j] == 1
+        assert np.max(_rel(res.Y[esc], d["Y"][j][esc])) <= 10 * rtol
+        same_steps.append(np.mean(res.n_steps == d["n_steps"][j]))
+    assert np.mean(same_steps) > 0.9
+
+
+def test_empty_batch_and_input_errors() -> None:
+    be = K.CudaBackend()
+    st = K.Spacetime(1.0, 0.9)
+    res = be.integrate_batch(st, np.zeros((0, 8)), K.IntegratorOptions(), K.TerminationOptions())
+    assert res.Y.shape == (0, 8) and res.state.shape == (0,)
+    with pytest.raises(ValueError):
+        be.integrate_batch(st, np.ones((2, 7)), K.IntegratorOptions(), K.TerminationOptions())
+    bad = np.ones((1, 8))
+    bad[0, 0] = np.nan
+    with pytest.raises(ValueError):
+        be.integrate_batch(st, bad, K.IntegratorOptions(), K.TerminationOptions())
+    with pytest.raises(ValueError):
+        be.integrate_batch(st, np.ones((1, 8)), K.IntegratorOptions(method="dop853"), K.TerminationOptions())
+    with pytest.raises(ValueError):
+        K.CudaBackend(precision="mixed").integrate_batch(st, np.ones((1, 8)), K.IntegratorOptions(method="rk4"),
+                                                         K.TerminationOptions())
+    with pytest.raises(ValueError):
+        K.initial_states(K.Camera(radius=1.5, inclination_deg=60.0, fov=0.1, resolution=2), st)
