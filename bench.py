@@ -49,6 +49,25 @@ def algorithmic_flops(stats: dict) -> float:
     return FLOP_PER_ATTEMPT * stats["attempts"] + FLOP_PER_ACCEPT * stats["accepted"] + FLOP_PER_RAY * stats["photons"]
 
 
+WORKLOADS = {
+    "sweep": WORKLOAD,
+    "sweep128": "the 36 128^2 images of the sweep (a*{0,0.5,0.9,0.99} x i{17,60,85} x rtol{1e-6,1e-8,1e-10})",
+    "spin99_1024": "a*=0.99, i=85deg, r_o=1000 M, +-8 M, 1024^2, rtol 1e-6, atol 1e-8",
+}
+
+
+def workload_specs(K, name: str):
+    if name == "sweep":
+        return sweep_specs(K)
+    if name == "sweep128":
+        return sweep_specs(K, resolutions=(128,))
+    if name == "spin99_1024":
+        cam = K.Camera(radius=1000.0, inclination_deg=85.0, fov=8.0, resolution=1024)
+        integ = K.IntegratorOptions(method="rk45", rtol=1e-6, atol=1e-8)
+        return [K.ImageSpec(K.Spacetime(1.0, 0.99), cam, integ, K.TerminationOptions())]
+    raise ValueError(name)
+
+
 def sweep_specs(K, resolutions=(128, 256, 512)):
     specs = []
     for spin in (0.0, 0.5, 0.9, 0.99):
@@ -230,9 +249,9 @@ def run_ours(args) -> None:
     K.trace_images  # noqa: B018 (import check)
     _lib.lib()
 
-    specs = sweep_specs(K)
+    specs = workload_specs(K, args.workload)
     total = sum(s.n_rays for s in specs)
-    sweep = K.DeviceSweep(specs, precision="fast64", device=local)
+    sweep = K.DeviceSweep(specs, precision=args.precision, device=local)
     stream = torch.cuda.current_stream(local)
     for _ in range(args.warmup):
         sweep.run()
@@ -275,7 +294,7 @@ def run_ours(args) -> None:
 
     extra = {}
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.kernel_only:
         # Plain FP64 (one thread per photon, reference operation order) on the same images.
         plain = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True))
         plain.run()
@@ -299,11 +318,11 @@ def run_ours(args) -> None:
         outs["event_hit"] = None
         del sweep
         torch.cuda.empty_cache()
-        K.trace_images(specs, precision="fast64", Y0=y0, out=outs, device=local)
+        K.trace_images(specs, precision=args.precision, Y0=y0, out=outs, device=local)
         e2e_steps = max(1, min(args.steps, 3))
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            K.trace_images(specs, precision="fast64", Y0=y0, out=outs, device=local)
+            K.trace_images(specs, precision=args.precision, Y0=y0, out=outs, device=local)
         e2e_s = (time.perf_counter() - t0) / e2e_steps
         d2h = sum(a.nbytes for a in outs.values() if a is not None)
         e2e = {"value": world * total / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": int(y0.nbytes),
@@ -312,13 +331,14 @@ def run_ours(args) -> None:
         extra["state_counts"] = {n: int(c) for n, c in zip(
             ("RUNNING", "ESCAPED", "CAPTURED", "MAX_AFFINE", "FAILURE", "OUT_OF_DOMAIN", "DISK_HIT"), counts)}
 
-    cpu = cpu_baseline(specs) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    cpu = cpu_baseline(specs) if (rank == 0 and world == 1 and not args.no_cpu and not args.kernel_only) else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "photons": total, "images": len(specs), "precision": "fast64",
+            "config": {"workload": WORKLOADS[args.workload], "photons": total, "images": len(specs),
+                       "precision": args.precision,
                        "kernel": "persistent work queue", "parallelism": f"replicas{world}",
                        "l2": "256 MB buffer written between timed steps (> 126 MB L2)"},
             "e2e": e2e, "gpu_launches": args.steps,
@@ -343,6 +363,10 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sweep")
+    ap.add_argument("--precision", choices=("reference", "fast64", "mixed"), default="fast64")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time the device launches only (no plain-kernel, end-to-end or CPU legs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

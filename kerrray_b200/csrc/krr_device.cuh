@@ -425,6 +425,10 @@ __device__ __forceinline__ typename M::N step_factor(typename M::N en, bool reje
     N raw;
     if constexpr (M::kFastFactor) {
       raw = (N)(0.9f * exp2f(-0.2f * __log2f((float)en)));
+    } else if constexpr (sizeof(N) == 4) {
+      // float32 working precision: the power evaluated in double and rounded once to float,
+      // i.e. the correctly rounded powf of the reference's float32 ** float32.
+      raw = (N)SAFETY * (N)pow((double)en, (double)(N)ERROR_EXPONENT);
     } else {
       raw = (N)SAFETY * pow(en, (N)ERROR_EXPONENT);
     }
