@@ -119,8 +119,15 @@ typedef struct krr_launch {
   int32_t blocks_per_sm;     /* resident blocks per SM */
   int32_t refill_threshold;  /* idle lanes of a warp before it refills from the queue */
   int32_t plain;             /* 1: one thread per photon, no work queue (the plain kernel) */
-  int32_t reserved;
+  int32_t variant;           /* compiled launch shape of the persistent kernel (krr_list_variants) */
 } krr_launch;
+
+/* A compiled launch shape of the persistent kernel: threads per block and the launch-bounds
+ * minimum of resident blocks per SM (its register cap), with the registers and the resident
+ * blocks per SM the device reports. */
+typedef struct krr_variant_info {
+  int32_t block, min_blocks, registers, blocks_per_sm;
+} krr_variant_info;
 
 /* Counters of a batched launch. */
 typedef struct krr_stats {
@@ -167,6 +174,12 @@ KRR_API int krr_trace_images(int device, const krr_image* images, int32_t n_imag
  * krr_workspace_size(n_images) bytes of device memory owned by the caller; stream as above.
  * Synchronises the stream before returning (the statistics are read back). */
 KRR_API size_t krr_workspace_size(int32_t n_images);
+
+/* The launch shapes compiled for (precision, options.method, options.dtype): *count receives
+ * their number; up to max_out are described in out (nullable) for `device`.  Measurement
+ * support for the autotuner; no counterpart in the reference. */
+KRR_API int krr_list_variants(int device, int32_t precision, const krr_options* options, krr_variant_info* out,
+                              int32_t max_out, int32_t* count);
 KRR_API int krr_trace_images_device(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
                             const krr_launch* launch, const krr_result* d_out, void* workspace,
                             void* stream, krr_stats* stats);

@@ -6,6 +6,7 @@ C++ behind the C ABI of ``include/kerrray_cuda.h``); this package is the host si
 """
 
 from kerrray_b200._lib import BackendUnavailable
+from kerrray_b200.autotune import autotune, list_variants
 from kerrray_b200.backends import (
     BACKEND_NAMES,
     Backend,
@@ -32,7 +33,7 @@ from kerrray_b200.types import (
 __all__ = [
     "BACKEND_NAMES", "Backend", "BackendUnavailable", "BatchResult", "Camera", "CudaBackend", "DeviceSweep",
     "EventOptions", "FAILURE_STATES", "ImageSpec", "IntegratorOptions", "LaunchConfig", "ShadowImage", "Spacetime",
-    "SweepResult", "TerminationOptions", "TerminationState", "available_backends", "compute_shadow",
-    "concatenate_results", "get_backend", "initial_states", "initial_states_at", "max_attempts", "order_by_cost",
+    "SweepResult", "TerminationOptions", "TerminationState", "autotune", "available_backends", "compute_shadow",
+    "concatenate_results", "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
     "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
 ]

@@ -25,7 +25,7 @@ PRECISIONS = {"reference": 0, "fast64": 1, "mixed": 2}
 EXPORTS = (
     "krr_last_error", "krr_abi_version", "krr_device_count", "krr_max_attempts", "krr_integrate_batch",
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
-    "krr_trace_images_device", "krr_fma_peak",
+    "krr_trace_images_device", "krr_fma_peak", "krr_list_variants",
 )
 
 
@@ -62,7 +62,12 @@ class KrrImage(ctypes.Structure):
 
 class KrrLaunch(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("refill_threshold", ctypes.c_int32), ("plain", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("refill_threshold", ctypes.c_int32), ("plain", ctypes.c_int32), ("variant", ctypes.c_int32)]
+
+
+class KrrVariantInfo(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int32), ("min_blocks", ctypes.c_int32), ("registers", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32)]
 
 
 class KrrStats(ctypes.Structure):
@@ -116,6 +121,9 @@ def lib() -> ctypes.CDLL:
         L.krr_trace_images_device.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
                                               ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp, vp,
                                               ctypes.POINTER(KrrStats)]
+        L.krr_list_variants.restype = ctypes.c_int
+        L.krr_list_variants.argtypes = [ctypes.c_int, i32, ctypes.POINTER(KrrOptions), ctypes.POINTER(KrrVariantInfo),
+                                        i32, ctypes.POINTER(ctypes.c_int32)]
         L.krr_fma_peak.restype = ctypes.c_int
         L.krr_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         _LIB = L

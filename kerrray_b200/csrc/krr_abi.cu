@@ -333,20 +333,29 @@ int build_images(const krr_image* images, int32_t n_images, std::vector<krr::Ima
 }
 
 struct LaunchShape {
-  int block, grid, refill;
+  const krr::Variant* v;
+  int grid, refill;
 };
 
-LaunchShape persistent_shape(int device, int32_t precision, const krr_options* o, const krr_launch* l) {
-  LaunchShape s{};
-  s.block = (l && l->block > 0) ? l->block : 128;
+const krr::Variant* variants_for(int32_t precision, const krr_options* o, int* count) {
   const bool rk4 = o->method == 1;
-  int occ = precision == KRR_PREC_REFERENCE ? krr::ref_occupancy(o->dtype == 1, rk4, true, s.block)
-                                            : krr::fast_occupancy(precision == KRR_PREC_MIXED, rk4, true, s.block);
-  if (occ < 1) occ = 1;
-  int bps = (l && l->blocks_per_sm > 0) ? std::min(l->blocks_per_sm, occ) : occ;
+  if (precision == KRR_PREC_REFERENCE) return krr::ref_variants(o->dtype == 1, rk4, count);
+  return krr::fast_variants(precision == KRR_PREC_MIXED, rk4, count);
+}
+
+int persistent_shape(int device, int32_t precision, const krr_options* o, const krr_launch* l, LaunchShape& s) {
+  int count = 0;
+  const krr::Variant* vs = variants_for(precision, o, &count);
+  if (!vs || count < 1) return fail(KRR_ERR_UNSUPPORTED, "no persistent kernel for this precision/method");
+  const int idx = (l && l->variant > 0) ? l->variant : 0;
+  if (idx >= count) return fail(KRR_ERR_INVALID, "launch variant %d out of range [0, %d)", idx, count);
+  s.v = &vs[idx];
+  int occ = s.v->occupancy();
+  if (occ < 1) return fail(KRR_ERR_CUDA, "persistent kernel variant %d cannot be resident on this device", idx);
+  const int bps = (l && l->blocks_per_sm > 0) ? std::min(l->blocks_per_sm, occ) : occ;
   s.grid = sm_count_of(device) * bps;
   s.refill = (l && l->refill_threshold > 0) ? std::min(l->refill_threshold, 32) : 1;
-  return s;
+  return KRR_OK;
 }
 
 int run_images(Context* c, const krr_image* images, const std::vector<krr::Image>& ims, long long total,
@@ -363,7 +372,9 @@ int run_images(Context* c, const krr_image* images, const std::vector<krr::Image
   KRR_CUDA(cudaMemsetAsync(d_q, 0, sizeof(krr::Queue), s));
   if (d_out->event_Y) KRR_CUDA(cudaMemsetAsync(d_out->event_Y, 0, (size_t)total * 8 * sizeof(double), s));
   if (d_out->event_hit) KRR_CUDA(cudaMemsetAsync(d_out->event_hit, 0, (size_t)total, s));
-  const LaunchShape shape = persistent_shape(c->device, precision, o0, launch);
+  LaunchShape shape{};
+  rc = persistent_shape(c->device, precision, o0, launch, shape);
+  if (rc) return rc;
   krr::PersistArgs a{};
   a.images = d_images;
   a.n_images = (int)ims.size();
@@ -373,7 +384,7 @@ int run_images(Context* c, const krr_image* images, const std::vector<krr::Image
   a.q = d_q;
   a.refill_threshold = shape.refill;
   a.grid = shape.grid;
-  a.block = shape.block;
+  a.block = shape.v->block;
   const bool rk4 = o0->method == 1;
   const bool plain = launch && launch->plain;
   KRR_CUDA(cudaEventRecord(c->ev0, s));
@@ -390,10 +401,8 @@ int run_images(Context* c, const krr_image* images, const std::vector<krr::Image
       KRR_CUDA(krr::ref_plain(o0->dtype == 1, rk4, pa, block, s));
     else
       KRR_CUDA(krr::fast_plain(precision == KRR_PREC_MIXED, rk4, pa, block, s));
-  } else if (precision == KRR_PREC_REFERENCE) {
-    KRR_CUDA(krr::ref_persistent(o0->dtype == 1, rk4, a, s));
   } else {
-    KRR_CUDA(krr::fast_persistent(precision == KRR_PREC_MIXED, rk4, a, s));
+    KRR_CUDA(shape.v->run(a, s));
   }
   KRR_CUDA(cudaEventRecord(c->ev1, s));
   krr::Queue q{};
@@ -554,6 +563,29 @@ int krr_camera_states(int device, double mass, double spin, const krr_camera* ca
   KRR_CUDA(cudaMemcpyAsync(Y0, c->buf[B_Y0].p, (size_t)rows * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   KRR_CUDA(cudaStreamSynchronize(c->stream));
   if (err) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
+  return KRR_OK;
+}
+
+int krr_list_variants(int device, int32_t precision, const krr_options* options, krr_variant_info* out,
+                      int32_t max_out, int32_t* count) {
+  int rc = validate_options(options);
+  if (rc) return rc;
+  rc = check_precision(precision, options);
+  if (rc) return rc;
+  if (!count) return fail(KRR_ERR_INVALID, "count must not be NULL");
+  int n = 0;
+  const krr::Variant* vs = variants_for(precision, options, &n);
+  *count = n;
+  if (!out) return KRR_OK;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(KRR_ERR_NO_DEVICE, "no CUDA device available");
+  KRR_CUDA(cudaSetDevice(device));
+  for (int i = 0; i < n && i < max_out; ++i) {
+    out[i].block = vs[i].block;
+    out[i].min_blocks = vs[i].min_blocks;
+    out[i].registers = vs[i].registers();
+    out[i].blocks_per_sm = vs[i].occupancy();
+  }
   return KRR_OK;
 }
 

@@ -11,21 +11,35 @@ cudaError_t fast_plain(bool mixed, bool rk4, const PlainArgs& a, int block, cuda
   return rk4 ? run_plain<Fast64, true>(a, block, s) : run_plain<Fast64, false>(a, block, s);
 }
 
-cudaError_t fast_persistent(bool mixed, bool rk4, const PersistArgs& a, cudaStream_t s) {
+// Launch shapes the autotuner chooses from: (threads per block, minimum resident blocks per SM).
+// The minimum caps the registers at 65536 / (block * min_blocks): unbounded, 170, 128 and 102
+// for FP64; unbounded, 128, 102 and 85 for the mixed mode.
+const Variant* fast_variants(bool mixed, bool rk4, int* count) {
+  static const Variant f64[] = {
+      make_variant<Fast64, false, 128, 1>(), make_variant<Fast64, false, 128, 3>(),
+      make_variant<Fast64, false, 128, 4>(), make_variant<Fast64, false, 128, 5>(),
+      make_variant<Fast64, false, 256, 2>(), make_variant<Fast64, false, 64, 8>(),
+  };
+  static const Variant f64rk4[] = {make_variant<Fast64, true, 128, 1>()};
+  static const Variant mix[] = {
+      make_variant<Mixed, false, 128, 1>(), make_variant<Mixed, false, 128, 4>(),
+      make_variant<Mixed, false, 128, 5>(), make_variant<Mixed, false, 128, 6>(),
+      make_variant<Mixed, false, 256, 2>(), make_variant<Mixed, false, 64, 10>(),
+  };
   if (mixed) {
-    if (rk4) return cudaErrorNotSupported;
-    return run_persistent<Mixed, false>(a, s);
+    if (rk4) {
+      *count = 0;
+      return nullptr;
+    }
+    *count = (int)(sizeof(mix) / sizeof(mix[0]));
+    return mix;
   }
-  return rk4 ? run_persistent<Fast64, true>(a, s) : run_persistent<Fast64, false>(a, s);
-}
-
-int fast_occupancy(bool mixed, bool rk4, bool persistent, int block) {
-  if (persistent) {
-    if (mixed) return rk4 ? 0 : persistent_occupancy<Mixed, false>(block);
-    return rk4 ? persistent_occupancy<Fast64, true>(block) : persistent_occupancy<Fast64, false>(block);
+  if (rk4) {
+    *count = 1;
+    return f64rk4;
   }
-  if (mixed) return rk4 ? 0 : plain_occupancy<Mixed, false>(block);
-  return rk4 ? plain_occupancy<Fast64, true>(block) : plain_occupancy<Fast64, false>(block);
+  *count = (int)(sizeof(f64) / sizeof(f64[0]));
+  return f64;
 }
 
 }  // namespace krr

@@ -98,10 +98,12 @@ __global__ void k_trace_plain(Params P, const Image* __restrict__ images, int n_
   }
 }
 
-template <class M, bool RK4>
-__global__ void k_trace_persistent(const Image* __restrict__ images, int n_images, long long total,
-                                   const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q,
-                                   int refill_threshold) {
+// MAXT threads per block and MINB resident blocks per SM are the launch bounds: the register
+// cap (65536 / (MAXT * MINB)) that trades per-thread registers against resident warps.
+template <class M, bool RK4, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
+    k_trace_persistent(const Image* __restrict__ images, int n_images, long long total,
+                       const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q, int refill_threshold) {
   constexpr unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -210,20 +212,43 @@ cudaError_t run_plain(const PlainArgs& a, int block, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <class M, bool RK4>
+template <class M, bool RK4, int MAXT, int MINB>
 cudaError_t run_persistent(const PersistArgs& a, cudaStream_t s) {
   if (a.total <= 0) return cudaSuccess;
-  k_trace_persistent<M, RK4><<<a.grid, a.block, 0, s>>>(a.images, a.n_images, a.total, a.Y0, a.o, a.q,
-                                                         a.refill_threshold);
+  k_trace_persistent<M, RK4, MAXT, MINB><<<a.grid, MAXT, 0, s>>>(a.images, a.n_images, a.total, a.Y0, a.o, a.q,
+                                                                  a.refill_threshold);
   return cudaGetLastError();
 }
 
-template <class M, bool RK4>
-int persistent_occupancy(int block) {
+template <class M, bool RK4, int MAXT, int MINB>
+int persistent_occupancy() {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_persistent<M, RK4>, block, 0) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_persistent<M, RK4, MAXT, MINB>, MAXT, 0) !=
+      cudaSuccess)
     return 0;
   return nb;
+}
+
+template <class M, bool RK4, int MAXT, int MINB>
+int persistent_registers() {
+  cudaFuncAttributes attr{};
+  if (cudaFuncGetAttributes(&attr, k_trace_persistent<M, RK4, MAXT, MINB>) != cudaSuccess) return 0;
+  return attr.numRegs;
+}
+
+// A compiled launch shape of the persistent kernel.
+struct Variant {
+  int block;     // threads per block
+  int min_blocks;  // launch-bounds minimum resident blocks per SM (1 = no register cap)
+  cudaError_t (*run)(const PersistArgs&, cudaStream_t);
+  int (*occupancy)();
+  int (*registers)();
+};
+
+template <class M, bool RK4, int MAXT, int MINB>
+constexpr Variant make_variant() {
+  return Variant{MAXT, MINB, &run_persistent<M, RK4, MAXT, MINB>, &persistent_occupancy<M, RK4, MAXT, MINB>,
+                 &persistent_registers<M, RK4, MAXT, MINB>};
 }
 
 template <class M, bool RK4>

@@ -11,13 +11,11 @@ namespace krr {
 
 // Reference order: dtype32 selects the reference's float32 working precision.
 cudaError_t ref_plain(bool dtype32, bool rk4, const PlainArgs& a, int block, cudaStream_t s);
-cudaError_t ref_persistent(bool dtype32, bool rk4, const PersistArgs& a, cudaStream_t s);
-int ref_occupancy(bool dtype32, bool rk4, bool persistent, int block);
+const Variant* ref_variants(bool dtype32, bool rk4, int* count);
 
 // Fast modes: mixed selects FP32 stages with FP64 accumulation; otherwise FP64.
 cudaError_t fast_plain(bool mixed, bool rk4, const PlainArgs& a, int block, cudaStream_t s);
-cudaError_t fast_persistent(bool mixed, bool rk4, const PersistArgs& a, cudaStream_t s);
-int fast_occupancy(bool mixed, bool rk4, bool persistent, int block);
+const Variant* fast_variants(bool mixed, bool rk4, int* count);
 
 // Camera initial states for a pixel grid (alpha == beta == nullptr) or for points.
 cudaError_t camera_states(const Frame& F, double fov, long long res, const double* alpha, const double* beta,

@@ -10,19 +10,14 @@ cudaError_t ref_plain(bool dtype32, bool rk4, const PlainArgs& a, int block, cud
   return rk4 ? run_plain<RefMode<double>, true>(a, block, s) : run_plain<RefMode<double>, false>(a, block, s);
 }
 
-cudaError_t ref_persistent(bool dtype32, bool rk4, const PersistArgs& a, cudaStream_t s) {
-  if (dtype32)
-    return rk4 ? run_persistent<RefMode<float>, true>(a, s) : run_persistent<RefMode<float>, false>(a, s);
-  return rk4 ? run_persistent<RefMode<double>, true>(a, s) : run_persistent<RefMode<double>, false>(a, s);
-}
-
-int ref_occupancy(bool dtype32, bool rk4, bool persistent, int block) {
-  if (persistent) {
-    if (dtype32) return rk4 ? persistent_occupancy<RefMode<float>, true>(block) : persistent_occupancy<RefMode<float>, false>(block);
-    return rk4 ? persistent_occupancy<RefMode<double>, true>(block) : persistent_occupancy<RefMode<double>, false>(block);
-  }
-  if (dtype32) return rk4 ? plain_occupancy<RefMode<float>, true>(block) : plain_occupancy<RefMode<float>, false>(block);
-  return rk4 ? plain_occupancy<RefMode<double>, true>(block) : plain_occupancy<RefMode<double>, false>(block);
+const Variant* ref_variants(bool dtype32, bool rk4, int* count) {
+  static const Variant v64[] = {make_variant<RefMode<double>, false, 128, 1>()};
+  static const Variant v64rk4[] = {make_variant<RefMode<double>, true, 128, 1>()};
+  static const Variant v32[] = {make_variant<RefMode<float>, false, 128, 1>()};
+  static const Variant v32rk4[] = {make_variant<RefMode<float>, true, 128, 1>()};
+  *count = 1;
+  if (dtype32) return rk4 ? v32rk4 : v32;
+  return rk4 ? v64rk4 : v64;
 }
 
 // Camera kernel: one image point per thread.

@@ -52,10 +52,11 @@ class ImageSpec:
 class LaunchConfig:
     """Launch shape of the persistent kernel (0 = library default)."""
 
-    block: int = 0
-    blocks_per_sm: int = 0
-    refill_threshold: int = 0
-    plain: bool = False
+    block: int = 0            # threads per block of the plain kernel
+    blocks_per_sm: int = 0    # resident blocks per SM (0 = as many as fit)
+    refill_threshold: int = 0  # idle lanes before a warp refills (0 = 1)
+    plain: bool = False       # one thread per photon instead of the work queue
+    variant: int = 0          # compiled launch shape of the persistent kernel
 
 
 def order_by_cost(specs: Sequence[ImageSpec]) -> list[int]:
@@ -80,7 +81,7 @@ def _launch(precision: str, cfg: LaunchConfig | None) -> _lib.KrrLaunch:
         raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}, got {precision!r}")
     cfg = cfg or LaunchConfig()
     return _lib.KrrLaunch(precision=_lib.PRECISIONS[precision], block=cfg.block, blocks_per_sm=cfg.blocks_per_sm,
-                          refill_threshold=cfg.refill_threshold, plain=int(cfg.plain), reserved=0)
+                          refill_threshold=cfg.refill_threshold, plain=int(cfg.plain), variant=cfg.variant)
 
 
 @dataclass

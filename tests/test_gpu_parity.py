@@ -227,3 +227,31 @@ def test_empty_batch_and_input_errors() -> None:
                                                          K.TerminationOptions())
     with pytest.raises(ValueError):
         K.initial_states(K.Camera(radius=1.4, inclination_deg=60.0, fov=0.1, resolution=2), st)
+
+
+def test_every_launch_variant_gives_identical_results() -> None:
+    """Register caps and refill thresholds change the schedule, never the per-ray arithmetic."""
+    d = golden("shadow64_a0.9_i60")
+    st = K.Spacetime(1.0, 0.9)
+    cam = K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=64)
+    integ = K.IntegratorOptions(method="rk45", rtol=1e-6, atol=1e-8)
+    spec = K.ImageSpec(st, cam, integ, K.TerminationOptions())
+    for precision in ("fast64", "mixed"):
+        variants = K.list_variants(precision, integ, K.TerminationOptions())
+        assert len(variants) >= 4 and all(v["blocks_per_sm"] >= 1 for v in variants)
+        base = K.trace_images([spec], precision=precision, Y0=d["Y0"])
+        for v in variants:
+            for t in (1, 8):
+                sw = K.trace_images([spec], precision=precision, Y0=d["Y0"],
+                                    launch=K.LaunchConfig(variant=v["variant"], refill_threshold=t))
+                assert np.array_equal(sw.arrays["Y"], base.arrays["Y"]), (precision, v, t)
+                assert np.array_equal(sw.arrays["n_steps"], base.arrays["n_steps"])
+                assert sw.stats["retired"] == 4096
+
+
+def test_autotuner_picks_a_measured_candidate() -> None:
+    specs = [K.ImageSpec(K.Spacetime(1.0, a), K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=128),
+                         K.IntegratorOptions(rtol=1e-6, atol=1e-8), K.TerminationOptions()) for a in (0.0, 0.9)]
+    cfg, report = K.autotune(specs, precision="fast64", use_cache=False, thresholds=(1, 8), repeats=1)
+    assert report["trials"] and report["ms"] == min(t["ms"] for t in report["trials"])
+    assert (cfg.variant, cfg.refill_threshold) in {(t["variant"], t["refill_threshold"]) for t in report["trials"]}
