@@ -184,6 +184,23 @@ KRR_API int krr_trace_images_device(int device, const krr_image* images, int32_t
                             const krr_launch* launch, const krr_result* d_out, void* workspace,
                             void* stream, krr_stats* stats);
 
+/* Allocation-free form of krr_trace_images_device.  No counterpart in the reference.  For
+ * callers that cannot allocate device memory on this path (an application that owns a fixed
+ * device-memory budget, work enqueued on a stream another library captures, a plug-in whose
+ * host owns all device memory): the launch's scratch (work-queue counters and image
+ * descriptors) lives in a static array in the library's device image, sized for at most
+ * KRR_NOALLOC_MAX_IMAGES images (about 43 KB per device, held until exit); larger batches are
+ * rejected with KRR_ERR_INVALID.  Inputs (d_Y0, nullable) and outputs (d_out) are the caller's
+ * device buffers; nothing is allocated.  The first call on a device looks up the array's
+ * device address, so make that first call before any stream capture.  All calls share the
+ * one array (its counters are cleared at the start of each call): calls that overlap on the
+ * GPU race, so serialise them (one stream, or one call at a time).  Synchronises `stream`;
+ * kernel_ms is reported as 0. */
+#define KRR_NOALLOC_MAX_IMAGES 128
+KRR_API int krr_trace_images_noalloc(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
+                                     const krr_launch* launch, const krr_result* d_out, void* stream,
+                                     krr_stats* stats);
+
 /* Measurement utility with no counterpart in the reference (which reports no GPU number):
  * the FP64 (fp64 != 0) or FP32 FMA throughput of `device` in TFLOP/s (2 FLOP per FMA), from
  * dependent FMA chains timed with CUDA events; the roofline denominator of the step kernels. */

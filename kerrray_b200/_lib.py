@@ -25,7 +25,7 @@ PRECISIONS = {"reference": 0, "fast64": 1, "mixed": 2}
 EXPORTS = (
     "krr_last_error", "krr_abi_version", "krr_device_count", "krr_max_attempts", "krr_integrate_batch",
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
-    "krr_trace_images_device", "krr_fma_peak", "krr_list_variants",
+    "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
 )
 
 
@@ -121,6 +121,10 @@ def lib() -> ctypes.CDLL:
         L.krr_trace_images_device.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
                                               ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp, vp,
                                               ctypes.POINTER(KrrStats)]
+        L.krr_trace_images_noalloc.restype = ctypes.c_int
+        L.krr_trace_images_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
+                                               ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp,
+                                               ctypes.POINTER(KrrStats)]
         L.krr_list_variants.restype = ctypes.c_int
         L.krr_list_variants.argtypes = [ctypes.c_int, i32, ctypes.POINTER(KrrOptions), ctypes.POINTER(KrrVariantInfo),
                                         i32, ctypes.POINTER(ctypes.c_int32)]

@@ -29,6 +29,7 @@ UNITS = {
     "krr_fast.cu": [],
     "krr_abi.cu": [],
     "krr_peak.cu": [],
+    "krr_noalloc.cu": [],
 }
 
 

@@ -15,9 +15,10 @@
 #include <vector>
 
 #include "../../include/kerrray_cuda.h"
+#include "krr_host.h"
 #include "krr_launch.h"
 
-namespace {
+namespace krr_host {
 
 thread_local std::string g_last_error;
 
@@ -425,7 +426,9 @@ int run_images(Context* c, const krr_image* images, const std::vector<krr::Image
   return KRR_OK;
 }
 
-}  // namespace
+}  // namespace krr_host
+
+using namespace krr_host;
 
 extern "C" {
 
