@@ -178,11 +178,15 @@ def time_cpu_sample(specs, stride: int, offset: int = 0) -> tuple[int, float, in
 
 
 def calibrate_stride(specs, target_s: float) -> int:
+    """Stride whose sample takes about target_s seconds (probe samples grow until >= 1 s)."""
     total = sum(s.n_rays for s in specs)
-    probe = max(total // 3000, 1)
-    n, dt, _ = time_cpu_sample(specs, probe, 0)
-    rate = n / max(dt, 1e-6)
-    want = max(int(rate * target_s), 1)
+    stride = max(total // 3000, 1)
+    while True:
+        n, dt, _ = time_cpu_sample(specs, stride, 0)
+        if dt >= 1.0 or stride == 1:
+            break
+        stride = max(stride // 4, 1)
+    want = max(int(n / max(dt, 1e-6) * target_s), 1)
     return max(total // want, 1)
 
 
@@ -231,6 +235,58 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _timed_steps(sweep, steps: int, stream, flush) -> list[float]:
+    """CUDA-event time (ms) of each graph launch; L2 flushed before each, outside the events."""
+    import torch
+
+    out = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sweep.run(stats=False)
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def mixed_vs_plain(K, local: int, stream, flush) -> dict:
+    """Mixed persistent + FP64 re-trace against the plain FP64 kernel on the 1024^2, a*=0.99,
+    i=85 deg image (rtol 1e-6): rays/s of each and whether the two shadow masks are identical."""
+    import torch
+
+    specs = workload_specs(K, "spin99_1024")
+    total = specs[0].n_rays
+    tuned, _ = K.autotune(specs, precision="mixed", device=local)
+    mixed = K.DeviceSweep(specs, precision="mixed", device=local,
+                          launch=K.LaunchConfig(variant=tuned.variant, refill_threshold=tuned.refill_threshold,
+                                                retrace=True))
+    fast = K.DeviceSweep(specs, precision="fast64", device=local, launch=K.autotune(specs, precision="fast64", device=local)[0])
+    plain = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True))
+    for sw in (mixed, fast, plain):
+        sw.run()
+    t_mixed = min(_timed_steps(mixed, 3, stream, flush))
+    t_fast = min(_timed_steps(fast, 3, stream, flush))
+    t_plain = min(_timed_steps(plain, 2, stream, flush))
+    ms = mixed.stats()
+    same = bool(torch.equal(mixed.tensors["state"], plain.tensors["state"]))
+    differ = int((mixed.tensors["state"] != plain.tensors["state"]).sum().item())
+    esc = (plain.tensors["state"] == 1) & (mixed.tensors["state"] == 1)
+    rel = ((mixed.tensors["Y"] - plain.tensors["Y"]).abs() / plain.tensors["Y"].abs().clamp_min(1.0)).amax(dim=1)
+    out = {"workload": WORKLOADS["spin99_1024"], "photons": total,
+           "mixed_retrace_rays_s": total / (t_mixed * 1e-3), "fast64_rays_s": total / (t_fast * 1e-3),
+           "plain_fp64_rays_s": total / (t_plain * 1e-3), "speedup_mixed_vs_plain": t_plain / t_mixed,
+           "mask_identical": same, "pixels_differing": differ, "retraced": int(ms["retraced"]),
+           "escaped_max_rel_dY_vs_plain": float(rel[esc].max().item()),
+           "escaped_median_rel_dY_vs_plain": float(rel[esc].median().item()),
+           "mixed_launch": {"variant": tuned.variant, "refill_threshold": tuned.refill_threshold}}
+    for sw in (mixed, fast, plain):
+        sw.close()
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -246,7 +302,6 @@ def run_ours(args) -> None:
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-    K.trace_images  # noqa: B018 (import check)
     _lib.lib()
 
     specs = workload_specs(K, args.workload)
@@ -255,7 +310,7 @@ def run_ours(args) -> None:
     sweep = K.DeviceSweep(specs, precision=args.precision, device=local, launch=tuned)
     stream = torch.cuda.current_stream(local)
     for _ in range(args.warmup):
-        sweep.run()
+        sweep.run(stats=False)
     torch.cuda.synchronize()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2 (126 MB)
 
@@ -263,22 +318,14 @@ def run_ours(args) -> None:
         if world > 1:
             dist.barrier()
 
-    step_ms, stats_all = [], []
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            stats_all.append(sweep.run())
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
+        step_ms = _timed_steps(sweep, args.steps, stream, flush)
         torch.cuda.synchronize()
         barrier()
     clock = clocks.summary()
+    stats = sweep.stats()
     elapsed_ms = float(sum(step_ms))
     if world > 1:
         t = torch.tensor([elapsed_ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -286,24 +333,28 @@ def run_ours(args) -> None:
         elapsed_ms = float(t.item())
     value = world * total * args.steps / (elapsed_ms / 1e3)
 
-    # Roofline of the trace kernel: algorithmic FLOPs per launch over its event-timed duration.
-    kernel_ms = statistics.mean(s["kernel_ms"] for s in stats_all)
-    flops = statistics.mean(algorithmic_flops(s) for s in stats_all)
+    # Roofline of the trace kernel: algorithmic FLOPs per launch over its event-timed duration
+    # (each timed graph launch holds this one kernel and two small memsets).
+    kernel_ms = statistics.mean(step_ms)
+    flops = algorithmic_flops(stats)
     achieved = flops / (kernel_ms * 1e-3) / 1e12
     peak64 = _lib.fma_peak_tflops(local, True)
-    st0 = stats_all[-1]
 
     extra = {}
     e2e = None
     if rank == 0 and not args.kernel_only:
         # Plain FP64 (one thread per photon, reference operation order) on the same images.
         plain = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True))
-        plain.run()
-        ps = plain.run()
-        extra["plain_fp64_rays_s"] = total / (ps["kernel_ms"] * 1e-3)
-        extra["persistent_fp64_rays_s"] = total / (kernel_ms * 1e-3)
-        extra["speedup_persistent_vs_plain"] = extra["persistent_fp64_rays_s"] / extra["plain_fp64_rays_s"]
+        plain.run(stats=False)
+        t_plain = min(_timed_steps(plain, 1, stream, flush))
+        extra["plain_fp64_rays_s"] = total / (t_plain * 1e-3)
+        extra["persistent_rays_s"] = total / (kernel_ms * 1e-3)
+        extra["speedup_persistent_vs_plain"] = t_plain / kernel_ms
+        extra["mask_identical_persistent_vs_plain"] = bool(torch.equal(plain.tensors["state"], sweep.tensors["state"]))
+        plain.close()
         del plain
+        torch.cuda.empty_cache()
+        extra["mixed_vs_plain_1024"] = mixed_vs_plain(K, local, stream, flush)
         torch.cuda.empty_cache()
         # End to end through the public API: pinned host Y0 in, every result array out.
         y0 = torch.empty((total, 8), dtype=torch.float64, pin_memory=True).numpy()
@@ -317,6 +368,7 @@ def run_ours(args) -> None:
             ("max_lz_drift", (total,), torch.float64), ("max_carter_drift", (total,), torch.float64))}
         outs["event_Y"] = None
         outs["event_hit"] = None
+        sweep.close()
         del sweep
         torch.cuda.empty_cache()
         K.trace_images(specs, precision=args.precision, Y0=y0, out=outs, device=local, launch=tuned)
@@ -334,17 +386,16 @@ def run_ours(args) -> None:
 
     cpu = cpu_baseline(specs) if (rank == 0 and world == 1 and not args.no_cpu and not args.kernel_only) else None
     if rank == 0:
+        chosen = [t for t in tune_report["trials"] if t["variant"] == tuned.variant
+                  and t["refill_threshold"] == tuned.refill_threshold][0]
         line = {
             "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload], "photons": total, "images": len(specs),
-                       "precision": args.precision,
-                       "kernel": "persistent work queue", "parallelism": f"replicas{world}",
-                       "launch": {k: v for k, v in [t for t in tune_report["trials"]
-                                                         if t["variant"] == tuned.variant
-                                                         and t["refill_threshold"] == tuned.refill_threshold][0].items()
-                                  if k != "ms"},
+                       "precision": args.precision, "kernel": "persistent work queue, CUDA-graph launch",
+                       "parallelism": f"replicas{world}",
+                       "launch": {k: v for k, v in chosen.items() if k != "ms"},
                        "l2": "256 MB buffer written between timed steps (> 126 MB L2)"},
             "e2e": e2e, "gpu_launches": args.steps,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
@@ -352,8 +403,8 @@ def run_ours(args) -> None:
                          "peak_source": "measured FP64 FMA chains on this device (krr_fma_peak)",
                          "algorithmic_flop_per_launch": flops, "kernel_ms": kernel_ms},
             "cpu_baseline": cpu, "clocks": clock,
-            "queue": {"attempts": st0["attempts"], "accepted": st0["accepted"],
-                      "lane_occupancy": st0["busy_slots"] / max(st0["lane_slots"], 1)},
+            "queue": {"attempts": stats["attempts"], "accepted": stats["accepted"],
+                      "lane_occupancy": stats["busy_slots"] / max(stats["lane_slots"], 1)},
             **extra,
         }
         print(json.dumps(line), flush=True)

@@ -120,6 +120,11 @@ typedef struct krr_launch {
   int32_t refill_threshold;  /* idle lanes of a warp before it refills from the queue */
   int32_t plain;             /* 1: one thread per photon, no work queue (the plain kernel) */
   int32_t variant;           /* compiled launch shape of the persistent kernel (krr_list_variants) */
+  int32_t retrace;           /* 1: after the trace, flag every pixel that did not end ESCAPED or
+                                CAPTURED or whose code differs from one of its 8 neighbours, and
+                                trace those again with the reference-order FP64 kernel (rk45,
+                                float64, persistent launches) */
+  int32_t reserved;
 } krr_launch;
 
 /* A compiled launch shape of the persistent kernel: threads per block and the launch-bounds
@@ -138,6 +143,9 @@ typedef struct krr_stats {
   uint64_t lane_slots;  /* warp iterations x 32 */
   uint64_t busy_slots;  /* lane slots that advanced a running photon */
   double kernel_ms;     /* device time of the trace kernel (CUDA events on its stream) */
+  uint64_t retraced;    /* photons traced again in FP64 (retrace on) */
+  uint64_t retrace_attempts;
+  double retrace_ms;    /* device time of the flagging and the re-trace */
 } krr_stats;
 
 KRR_API const char* krr_last_error(void);
@@ -170,10 +178,11 @@ KRR_API int krr_camera_states(int device, double mass, double spin, const krr_ca
 KRR_API int krr_trace_images(int device, const krr_image* images, int32_t n_images, const double* Y0,
                      const krr_launch* launch, const krr_result* out, krr_stats* stats);
 
-/* Device form of krr_trace_images: d_Y0 (nullable) and d_out on `device`; `workspace` is
- * krr_workspace_size(n_images) bytes of device memory owned by the caller; stream as above.
- * Synchronises the stream before returning (the statistics are read back). */
-KRR_API size_t krr_workspace_size(int32_t n_images);
+/* Device form of krr_trace_images: d_Y0 (nullable) and d_out on `device`; `workspace` is at
+ * least krr_workspace_size(n_images, retrace ? total photons : 0) bytes of device memory owned
+ * by the caller; stream as above.  Synchronises the stream before returning (the statistics
+ * are read back). */
+KRR_API size_t krr_workspace_size(int32_t n_images, int64_t retrace_photons);
 
 /* The launch shapes compiled for (precision, options.method, options.dtype): *count receives
  * their number; up to max_out are described in out (nullable) for `device`.  Measurement
@@ -182,7 +191,23 @@ KRR_API int krr_list_variants(int device, int32_t precision, const krr_options* 
                               int32_t max_out, int32_t* count);
 KRR_API int krr_trace_images_device(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
                             const krr_launch* launch, const krr_result* d_out, void* workspace,
-                            void* stream, krr_stats* stats);
+                            size_t workspace_bytes, void* stream, krr_stats* stats);
+
+/* A batched launch captured once as a CUDA graph and replayed: krr_plan_create uploads the
+ * image descriptors into `workspace` (krr_workspace_size bytes, caller-owned, like the outputs
+ * and d_Y0 it must outlive the plan) and captures the whole launch sequence (counter resets,
+ * persistent trace, and with retrace the flagging and FP64 re-trace, whose size is read on the
+ * device); krr_plan_launch enqueues it on `stream` without synchronising; krr_plan_stats
+ * synchronises `stream` and reads the counters of the last launch (kernel times 0: time the
+ * launches with events on your stream).  Replaces compute_shadow
+ * (src/kerrray/raytracing/shadow.py:179-211) repeated over the same images. */
+typedef struct krr_plan krr_plan;
+KRR_API int krr_plan_create(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
+                            const krr_launch* launch, const krr_result* d_out, void* workspace,
+                            size_t workspace_bytes, krr_plan** plan);
+KRR_API int krr_plan_launch(krr_plan* plan, void* stream);
+KRR_API int krr_plan_stats(krr_plan* plan, void* stream, krr_stats* stats);
+KRR_API int krr_plan_destroy(krr_plan* plan);
 
 /* Allocation-free form of krr_trace_images_device.  No counterpart in the reference.  For
  * callers that cannot allocate device memory on this path (an application that owns a fixed

@@ -26,6 +26,7 @@ EXPORTS = (
     "krr_last_error", "krr_abi_version", "krr_device_count", "krr_max_attempts", "krr_integrate_batch",
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
     "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
+    "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy",
 )
 
 
@@ -62,7 +63,8 @@ class KrrImage(ctypes.Structure):
 
 class KrrLaunch(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("refill_threshold", ctypes.c_int32), ("plain", ctypes.c_int32), ("variant", ctypes.c_int32)]
+                ("refill_threshold", ctypes.c_int32), ("plain", ctypes.c_int32), ("variant", ctypes.c_int32),
+                ("retrace", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class KrrVariantInfo(ctypes.Structure):
@@ -73,7 +75,8 @@ class KrrVariantInfo(ctypes.Structure):
 class KrrStats(ctypes.Structure):
     _fields_ = [("photons", ctypes.c_uint64), ("retired", ctypes.c_uint64), ("attempts", ctypes.c_uint64),
                 ("accepted", ctypes.c_uint64), ("lane_slots", ctypes.c_uint64), ("busy_slots", ctypes.c_uint64),
-                ("kernel_ms", ctypes.c_double)]
+                ("kernel_ms", ctypes.c_double), ("retraced", ctypes.c_uint64), ("retrace_attempts", ctypes.c_uint64),
+                ("retrace_ms", ctypes.c_double)]
 
     def as_dict(self) -> dict[str, Any]:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -116,11 +119,20 @@ def lib() -> ctypes.CDLL:
         L.krr_trace_images.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp, ctypes.POINTER(KrrLaunch),
                                        ctypes.POINTER(KrrResult), ctypes.POINTER(KrrStats)]
         L.krr_workspace_size.restype = ctypes.c_size_t
-        L.krr_workspace_size.argtypes = [i32]
+        L.krr_workspace_size.argtypes = [i32, i64]
         L.krr_trace_images_device.restype = ctypes.c_int
         L.krr_trace_images_device.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
-                                              ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp, vp,
-                                              ctypes.POINTER(KrrStats)]
+                                              ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp,
+                                              ctypes.c_size_t, vp, ctypes.POINTER(KrrStats)]
+        L.krr_plan_create.restype = ctypes.c_int
+        L.krr_plan_create.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp, ctypes.POINTER(KrrLaunch),
+                                      ctypes.POINTER(KrrResult), vp, ctypes.c_size_t, ctypes.POINTER(vp)]
+        L.krr_plan_launch.restype = ctypes.c_int
+        L.krr_plan_launch.argtypes = [vp, vp]
+        L.krr_plan_stats.restype = ctypes.c_int
+        L.krr_plan_stats.argtypes = [vp, vp, ctypes.POINTER(KrrStats)]
+        L.krr_plan_destroy.restype = ctypes.c_int
+        L.krr_plan_destroy.argtypes = [vp]
         L.krr_trace_images_noalloc.restype = ctypes.c_int
         L.krr_trace_images_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
                                                ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp,

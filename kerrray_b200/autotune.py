@@ -100,7 +100,7 @@ def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: i
             continue
         for t in thresholds:
             cfg = LaunchConfig(variant=v["variant"], refill_threshold=t)
-            sweep = DeviceSweep(small, precision=precision, launch=cfg, device=device, minimal=True)
+            sweep = DeviceSweep(small, precision=precision, launch=cfg, device=device, minimal=True, graph=False)
             sweep.run()
             ms = min(sweep.run()["kernel_ms"] for _ in range(repeats))
             trials.append({**v, "refill_threshold": t, "ms": ms})

@@ -2,8 +2,10 @@
 
 ``python -m kerrray_b200.build`` compiles each translation unit of ``csrc/`` with nvcc
 (``-gencode arch=compute_100a,code=sm_100a``, static CUDA runtime) and links them into one
-shared library that exports the C ABI of ``include/kerrray_cuda.h``. ``krr_ref.cu`` is
-compiled with ``-fmad=false`` (reference operation order, no contraction); the others contract.
+shared library that exports the C ABI of ``include/kerrray_cuda.h``. The kernel translation
+units are compiled with ``-fmad=false``: ``krr_ref.cu`` keeps the reference's rounding of every
+product and sum, ``krr_fast.cu`` writes its FMAs explicitly, so no result depends on how the
+compiler schedules a particular launch variant.
 Rebuilds only when a source or header is newer than the library.
 """
 
@@ -26,7 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-I", str(ROOT / "include"), "--expt-relaxed-constexpr"]
 UNITS = {
     "krr_ref.cu": ["-fmad=false"],
-    "krr_fast.cu": [],
+    "krr_fast.cu": ["-fmad=false"],
     "krr_abi.cu": [],
     "krr_peak.cu": [],
     "krr_noalloc.cu": [],

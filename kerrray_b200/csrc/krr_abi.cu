@@ -192,7 +192,7 @@ struct Context {
   std::mutex mu;
   int device = -1;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   int sm_count = 0;
   DevBuf buf[B_COUNT];
 };
@@ -215,6 +215,7 @@ int get_context(int device, Context** out) {
     KRR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     KRR_CUDA(cudaEventCreate(&c->ev0));
     KRR_CUDA(cudaEventCreate(&c->ev1));
+    KRR_CUDA(cudaEventCreate(&c->ev2));
     KRR_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
     g_ctx[device] = std::move(c);
   }
@@ -359,76 +360,187 @@ int persistent_shape(int device, int32_t precision, const krr_options* o, const 
   return KRR_OK;
 }
 
-int run_images(Context* c, const krr_image* images, const std::vector<krr::Image>& ims, long long total,
-               const double* d_Y0, const krr_launch* launch, const krr_result* d_out, void* d_work, cudaStream_t s,
-               krr_stats* stats) {
+// Device layout of a batched launch's workspace: the main and the re-trace queue counters, the
+// image descriptors, then the re-trace list (one int64 per photon when the re-trace is on).
+struct WorkLayout {
+  krr::Queue* q0;
+  krr::Queue* q1;
+  krr::Image* images;
+  long long* list;
+};
+
+constexpr size_t round256(size_t x) { return (x + 255) / 256 * 256; }
+
+size_t work_bytes(int n_images, long long list_entries) {
+  return 512 + round256((size_t)std::max(n_images, 0) * sizeof(krr::Image)) + (size_t)std::max(list_entries, 0LL) * 8;
+}
+
+WorkLayout work_layout(void* base, int n_images) {
+  char* b = static_cast<char*>(base);
+  WorkLayout w;
+  w.q0 = reinterpret_cast<krr::Queue*>(b);
+  w.q1 = reinterpret_cast<krr::Queue*>(b + 256);
+  w.images = reinterpret_cast<krr::Image*>(b + 512);
+  w.list = reinterpret_cast<long long*>(b + 512 + round256((size_t)n_images * sizeof(krr::Image)));
+  return w;
+}
+
+// Everything a batched launch enqueues, resolved and validated up front.
+struct Pipeline {
+  int device = 0;
+  int n_images = 0;
+  long long total = 0;
+  bool plain = false;
+  int plain_block = 128;
+  int32_t precision = KRR_PREC_FAST64;
+  bool dtype32 = false, rk4 = false, disk = false;
+  bool retrace = false;
+  WorkLayout w{};
+  krr_result out{};
+  krr::PersistArgs main{};
+  const krr::Variant* main_v = nullptr;
+  krr::PersistArgs re{};
+  const krr::Variant* re_v = nullptr;
+};
+
+int prepare_pipeline(int device, const krr_image* images, int n_images, long long total, const double* d_Y0,
+                     const krr_launch* launch, const krr_result* d_out, void* d_work, size_t work_size, Pipeline& p) {
   const int32_t precision = launch ? launch->precision : KRR_PREC_FAST64;
   const krr_options* o0 = &images[0].options;
   int rc = check_precision(precision, o0);
   if (rc) return rc;
-  const size_t qbytes = (sizeof(krr::Queue) + 255) / 256 * 256;
-  krr::Queue* d_q = static_cast<krr::Queue*>(d_work);
-  krr::Image* d_images = reinterpret_cast<krr::Image*>(static_cast<char*>(d_work) + qbytes);
-  KRR_CUDA(cudaMemcpyAsync(d_images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, s));
-  KRR_CUDA(cudaMemsetAsync(d_q, 0, sizeof(krr::Queue), s));
-  if (d_out->event_Y) KRR_CUDA(cudaMemsetAsync(d_out->event_Y, 0, (size_t)total * 8 * sizeof(double), s));
-  if (d_out->event_hit) KRR_CUDA(cudaMemsetAsync(d_out->event_hit, 0, (size_t)total, s));
+  p.device = device;
+  p.n_images = n_images;
+  p.total = total;
+  p.precision = precision;
+  p.dtype32 = o0->dtype == 1;
+  p.rk4 = o0->method == 1;
+  p.disk = o0->disk_plane != 0;
+  p.plain = launch && launch->plain;
+  p.plain_block = (launch && launch->block > 0 && launch->block % 32 == 0) ? launch->block : 128;
+  p.retrace = launch && launch->retrace;
+  if (p.retrace && (p.rk4 || p.dtype32 || p.plain))
+    return fail(KRR_ERR_UNSUPPORTED, "the FP64 re-trace follows persistent rk45 float64 launches only");
+  const size_t need = work_bytes(n_images, p.retrace ? total : 0);
+  if (work_size < need) return fail(KRR_ERR_INVALID, "workspace of %zu bytes is smaller than the %zu needed", work_size, need);
+  p.w = work_layout(d_work, n_images);
+  p.out = *d_out;
   LaunchShape shape{};
-  rc = persistent_shape(c->device, precision, o0, launch, shape);
+  rc = persistent_shape(device, precision, o0, launch, shape);
   if (rc) return rc;
-  krr::PersistArgs a{};
-  a.images = d_images;
-  a.n_images = (int)ims.size();
-  a.total = total;
-  a.Y0 = d_Y0;
-  a.o = to_outputs(d_out);
-  a.q = d_q;
-  a.refill_threshold = shape.refill;
-  a.grid = shape.grid;
-  a.block = shape.v->block;
-  const bool rk4 = o0->method == 1;
-  const bool plain = launch && launch->plain;
-  KRR_CUDA(cudaEventRecord(c->ev0, s));
-  if (plain) {
-    krr::PlainArgs pa{};
-    pa.images = d_images;
-    pa.n_images = (int)ims.size();
-    pa.Y0 = d_Y0;
-    pa.n = total;
-    pa.o = a.o;
-    pa.q = d_q;
-    const int block = (launch->block > 0 && launch->block % 32 == 0) ? launch->block : 128;
-    if (precision == KRR_PREC_REFERENCE)
-      KRR_CUDA(krr::ref_plain(o0->dtype == 1, rk4, pa, block, s));
-    else
-      KRR_CUDA(krr::fast_plain(precision == KRR_PREC_MIXED, rk4, pa, block, s));
-  } else {
-    KRR_CUDA(shape.v->run(a, s));
+  p.main_v = shape.v;
+  p.main.images = p.w.images;
+  p.main.n_images = n_images;
+  p.main.total = total;
+  p.main.Y0 = d_Y0;
+  p.main.o = to_outputs(d_out);
+  p.main.q = p.w.q0;
+  p.main.refill_threshold = shape.refill;
+  p.main.grid = shape.grid;
+  p.main.block = shape.v->block;
+  if (p.retrace) {
+    LaunchShape rs{};
+    krr_launch rl{};
+    rl.precision = KRR_PREC_REFERENCE;
+    rc = persistent_shape(device, KRR_PREC_REFERENCE, o0, &rl, rs);
+    if (rc) return rc;
+    p.re_v = rs.v;
+    p.re = p.main;
+    p.re.q = p.w.q1;
+    p.re.grid = rs.grid;
+    p.re.block = rs.v->block;
+    p.re.refill_threshold = 1;
+    p.re.index = p.w.list;
+    p.re.d_total = &p.w.q0->flagged;
   }
-  KRR_CUDA(cudaEventRecord(c->ev1, s));
-  krr::Queue q{};
-  KRR_CUDA(cudaMemcpyAsync(&q, d_q, sizeof(q), cudaMemcpyDeviceToHost, s));
-  KRR_CUDA(cudaStreamSynchronize(s));
-  float ms = 0.0f;
-  KRR_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-  if (stats) {
-    stats->photons = (uint64_t)total;
-    stats->retired = q.retired;
-    stats->attempts = q.attempts;
-    stats->accepted = q.accepted;
-    stats->lane_slots = q.lane_iters;
-    stats->busy_slots = q.busy_iters;
-    stats->kernel_ms = ms;
-  }
-  if (q.error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
-  if (q.retired != (unsigned long long)total)
-    return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu photons retired of %lld", q.retired, total);
   return KRR_OK;
+}
+
+// The launch sequence (also what a plan captures): clear the counters, trace, and, with the
+// re-trace on, flag the edge and failed pixels and trace them again in reference-order FP64.
+// Events (nullable) bracket the main kernel (ev0, ev1) and the re-trace (ev1, ev2).
+cudaError_t enqueue_pipeline(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t ev2) {
+  cudaError_t e = cudaMemsetAsync(p.w.q0, 0, 512, s);
+  if (e == cudaSuccess && p.out.event_Y) e = cudaMemsetAsync(p.out.event_Y, 0, (size_t)p.total * 8 * sizeof(double), s);
+  if (e == cudaSuccess && p.out.event_hit) e = cudaMemsetAsync(p.out.event_hit, 0, (size_t)p.total, s);
+  if (e == cudaSuccess && ev0) e = cudaEventRecord(ev0, s);
+  if (e != cudaSuccess) return e;
+  if (p.plain) {
+    krr::PlainArgs pa{};
+    pa.images = p.w.images;
+    pa.n_images = p.n_images;
+    pa.Y0 = p.main.Y0;
+    pa.n = p.total;
+    pa.o = p.main.o;
+    pa.q = p.w.q0;
+    e = p.precision == KRR_PREC_REFERENCE ? krr::ref_plain(p.dtype32, p.rk4, pa, p.plain_block, s)
+                                          : krr::fast_plain(p.precision == KRR_PREC_MIXED, p.rk4, pa, p.plain_block, s);
+  } else {
+    e = p.main_v->run(p.main, s);
+  }
+  if (e == cudaSuccess && ev1) e = cudaEventRecord(ev1, s);
+  if (e == cudaSuccess && p.retrace) {
+    e = krr::flag_boundary(p.w.images, p.n_images, p.total, reinterpret_cast<const long long*>(p.out.state), p.w.list,
+                           p.w.q0, s);
+    if (e == cudaSuccess) e = p.re_v->run(p.re, s);
+  }
+  if (e == cudaSuccess && ev2) e = cudaEventRecord(ev2, s);
+  return e;
+}
+
+// Read the counters back (synchronises the stream) and check the queue's bookkeeping.
+int finish_pipeline(const Pipeline& p, cudaStream_t s, krr_stats* stats, cudaEvent_t ev0, cudaEvent_t ev1,
+                    cudaEvent_t ev2) {
+  krr::Queue q[2];
+  std::memset(q, 0, sizeof(q));
+  KRR_CUDA(cudaMemcpyAsync(&q[0], p.w.q0, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaMemcpyAsync(&q[1], p.w.q1, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.0f, ms2 = 0.0f;
+  if (ev0 && ev1) KRR_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  if (ev1 && ev2) KRR_CUDA(cudaEventElapsedTime(&ms2, ev1, ev2));
+  if (stats) {
+    stats->photons = (uint64_t)p.total;
+    stats->retired = q[0].retired;
+    stats->attempts = q[0].attempts;
+    stats->accepted = q[0].accepted;
+    stats->lane_slots = q[0].lane_iters;
+    stats->busy_slots = q[0].busy_iters;
+    stats->kernel_ms = ms;
+    stats->retraced = p.retrace ? q[0].flagged : 0;
+    stats->retrace_attempts = q[1].attempts;
+    stats->retrace_ms = p.retrace ? ms2 : 0.0;
+  }
+  if (q[0].error || q[1].error)
+    return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
+  if (q[0].retired != (unsigned long long)p.total)
+    return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu photons retired of %lld", q[0].retired, p.total);
+  if (p.retrace && q[1].retired != q[0].flagged)
+    return fail(KRR_ERR_CUDA, "re-trace inconsistency: %llu photons retired of %llu flagged", q[1].retired, q[0].flagged);
+  return KRR_OK;
+}
+
+int run_images(Context* c, const krr_image* images, const std::vector<krr::Image>& ims, long long total,
+               const double* d_Y0, const krr_launch* launch, const krr_result* d_out, void* d_work, size_t work_size,
+               cudaStream_t s, krr_stats* stats) {
+  Pipeline p;
+  int rc = prepare_pipeline(c->device, images, (int)ims.size(), total, d_Y0, launch, d_out, d_work, work_size, p);
+  if (rc) return rc;
+  KRR_CUDA(cudaMemcpyAsync(p.w.images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, s));
+  KRR_CUDA(enqueue_pipeline(p, s, c->ev0, c->ev1, c->ev2));
+  return finish_pipeline(p, s, stats, c->ev0, c->ev1, c->ev2);
 }
 
 }  // namespace krr_host
 
 using namespace krr_host;
+
+struct krr_plan {
+  int device;
+  Pipeline p;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
 
 extern "C" {
 
@@ -592,14 +704,11 @@ int krr_list_variants(int device, int32_t precision, const krr_options* options,
   return KRR_OK;
 }
 
-size_t krr_workspace_size(int32_t n_images) {
-  const size_t q = (sizeof(krr::Queue) + 255) / 256 * 256;
-  return q + (size_t)std::max(n_images, 0) * sizeof(krr::Image);
-}
+size_t krr_workspace_size(int32_t n_images, int64_t retrace_photons) { return work_bytes(n_images, retrace_photons); }
 
 int krr_trace_images_device(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
-                            const krr_launch* launch, const krr_result* d_out, void* workspace, void* stream,
-                            krr_stats* stats) {
+                            const krr_launch* launch, const krr_result* d_out, void* workspace, size_t workspace_bytes,
+                            void* stream, krr_stats* stats) {
   std::vector<krr::Image> ims;
   long long total = 0;
   int rc = build_images(images, n_images, ims, total);
@@ -610,7 +719,70 @@ int krr_trace_images_device(int device, const krr_image* images, int32_t n_image
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(c->mu);
   KRR_CUDA(cudaSetDevice(device));
-  return run_images(c, images, ims, total, d_Y0, launch, d_out, workspace, static_cast<cudaStream_t>(stream), stats);
+  return run_images(c, images, ims, total, d_Y0, launch, d_out, workspace, workspace_bytes,
+                    static_cast<cudaStream_t>(stream), stats);
+}
+
+int krr_plan_create(int device, const krr_image* images, int32_t n_images, const double* d_Y0, const krr_launch* launch,
+                    const krr_result* d_out, void* workspace, size_t workspace_bytes, krr_plan** plan) {
+  if (!plan) return fail(KRR_ERR_INVALID, "plan must not be NULL");
+  *plan = nullptr;
+  std::vector<krr::Image> ims;
+  long long total = 0;
+  int rc = build_images(images, n_images, ims, total);
+  if (rc) return rc;
+  if (!d_out || !d_out->Y || !d_out->state || !workspace) return fail(KRR_ERR_INVALID, "Y, state and workspace must not be NULL");
+  Context* c = nullptr;
+  rc = get_context(device, &c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  KRR_CUDA(cudaSetDevice(device));
+  auto pl = std::make_unique<krr_plan>();
+  pl->device = device;
+  rc = prepare_pipeline(device, images, n_images, total, d_Y0, launch, d_out, workspace, workspace_bytes, pl->p);
+  if (rc) return rc;
+  KRR_CUDA(cudaMemcpyAsync(pl->p.w.images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, c->stream));
+  KRR_CUDA(cudaStreamSynchronize(c->stream));
+  KRR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t e = enqueue_pipeline(pl->p, c->stream, nullptr, nullptr, nullptr);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return fail(KRR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e3 = cudaGraphInstantiate(&exec, graph, 0);
+  if (e3 != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail(KRR_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e3));
+  }
+  pl->graph = graph;
+  pl->exec = exec;
+  *plan = pl.release();
+  return KRR_OK;
+}
+
+int krr_plan_launch(krr_plan* plan, void* stream) {
+  if (!plan) return fail(KRR_ERR_INVALID, "plan must not be NULL");
+  KRR_CUDA(cudaSetDevice(plan->device));
+  KRR_CUDA(cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
+int krr_plan_stats(krr_plan* plan, void* stream, krr_stats* stats) {
+  if (!plan) return fail(KRR_ERR_INVALID, "plan must not be NULL");
+  KRR_CUDA(cudaSetDevice(plan->device));
+  return finish_pipeline(plan->p, static_cast<cudaStream_t>(stream), stats, nullptr, nullptr, nullptr);
+}
+
+int krr_plan_destroy(krr_plan* plan) {
+  if (!plan) return KRR_OK;
+  cudaSetDevice(plan->device);
+  if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  if (plan->graph) cudaGraphDestroy(plan->graph);
+  delete plan;
+  return KRR_OK;
 }
 
 int krr_trace_images(int device, const krr_image* images, int32_t n_images, const double* Y0, const krr_launch* launch,
@@ -636,8 +808,9 @@ int krr_trace_images(int device, const krr_image* images, int32_t n_images, cons
   krr_result dev;
   rc = device_results(c, total, out, images[0].options.disk_plane != 0, &dev);
   if (rc) return rc;
-  KRR_CUDA(c->buf[B_QUEUE].ensure(krr_workspace_size(n_images)));
-  rc = run_images(c, images, ims, total, d_Y0, launch, &dev, c->buf[B_QUEUE].p, c->stream, stats);
+  const size_t wbytes = work_bytes(n_images, (launch && launch->retrace) ? total : 0);
+  KRR_CUDA(c->buf[B_QUEUE].ensure(wbytes));
+  rc = run_images(c, images, ims, total, d_Y0, launch, &dev, c->buf[B_QUEUE].p, wbytes, c->stream, stats);
   if (rc) return rc;
   rc = copy_results_back(c, total, &dev, out);
   if (rc) return rc;

@@ -16,7 +16,7 @@
 //                    -fmad=false so that products and sums round separately as in the
 //                    reference's fastmath=False build);
 //   RefMode<float>   the reference's float32 working-precision mode (metric in FP64, cast);
-//   Fast64           FP64 with FMA contraction, sincos, three reciprocals instead of the
+//   Fast64           FP64 with explicit FMAs, sincos, three reciprocals instead of the
 //                    seventeen divisions, and a single-precision step-factor power;
 //   Mixed            FP32 stages (metric, right-hand side, stage sums, error estimate) with the
 //                    state accumulation y + h*sum(b_i k_i), Delta = r^2 - 2Mr + a^2 and the error
@@ -105,6 +105,7 @@ struct RefMode {
   using K = W;  // stage type
   using N = W;  // error-norm type
   static constexpr bool kFastFactor = false;
+  static constexpr bool kFused = false;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
 
@@ -178,6 +179,7 @@ struct Fast64 {
   using K = double;
   using N = double;
   static constexpr bool kFastFactor = true;
+  static constexpr bool kFused = true;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
 
@@ -223,7 +225,7 @@ struct Fast64 {
     double g4 = 0.0, g9 = 0.0, g14 = 0.0;
     if (pph != 0.0) {  // polar-axis guard
       const double is2 = 1.0 / s2;
-      g4 = (dlt - a2 * s2) * isd * is2;
+      g4 = fma(-a2, s2, dlt) * isd * is2;
       g9 = fma(-sig_r * isig2, is2, a2 * sd_r * isd2);
       g14 = fma(-fma(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
     }
@@ -243,6 +245,7 @@ struct Mixed {
   using K = float;
   using N = double;
   static constexpr bool kFastFactor = true;
+  static constexpr bool kFused = true;
 
   // The accepted state's diagnostics (Carter constant, axis test) use FP64 sine and cosine.
   __device__ static Trig accept_trig(double th, const Trig&) {
@@ -297,7 +300,7 @@ struct Mixed {
     float g4 = 0.0f, g9 = 0.0f, g14 = 0.0f;
     if (pph_d != 0.0) {
       const float is2 = 1.0f / s2;
-      g4 = (dlt - a2 * s2) * isd * is2;
+      g4 = fmaf(-a2, s2, dlt) * isd * is2;
       g9 = fmaf(-sig_r * isig2, is2, a2 * sd_r * isd2);
       g14 = fmaf(-fmaf(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
     }
@@ -438,6 +441,27 @@ __device__ __forceinline__ typename M::N step_factor(typename M::N en, bool reje
   return factor;
 }
 
+// a*x + acc: one fused operation in the fast modes, two roundings (the reference's order) in
+// the reference modes.  Contraction is never left to the compiler, so every launch variant of
+// a mode computes the same bits.
+__device__ __forceinline__ double fused(double a, double x, double acc) { return fma(a, x, acc); }
+__device__ __forceinline__ float fused(float a, float x, float acc) { return fmaf(a, x, acc); }
+
+template <class M, class X>
+__device__ __forceinline__ X madd(X acc, X a, X x) {
+  if constexpr (M::kFused) return fused(a, x, acc);
+  else return acc + a * x;
+}
+
+// y + h * acc, the state update of a stage.  The mixed mode forms h * acc exactly in FP64 (a
+// product of two floats) and rounds once when adding it to the FP64 state.
+template <class M>
+__device__ __forceinline__ typename M::S upd(typename M::S y, typename M::K h, typename M::K acc) {
+  using S = typename M::S;
+  if constexpr (!M::kFused) return y + (S)(h * acc);
+  else return fused((S)h, (S)acc, y);
+}
+
 // One step attempt (numba_kernel.py:376-455): DP5(4) (or RK4) step, error norm, controller,
 // accept/reject, diagnostics and classification.  Returns with ry.state updated.
 template <class M, bool RK4>
@@ -459,46 +483,57 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   S ys[NV], yn[NV];
   Trig tr;
   const K* k0 = ry.f;
+  // Stage inputs: the reference's sums (same terms and order, zero coefficients skipped);
+  // madd / upd fuse them in the fast modes and round each operation in the reference modes.
+  auto c = [](double x) { return (K)x; };
   if constexpr (!RK4) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)dp::A10 * k0[i]));
+    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(dp::A10) * k0[i]);
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k1, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)dp::A20 * k0[i] + (K)dp::A21 * k1[i]));
+    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, madd<M>(c(dp::A20) * k0[i], c(dp::A21), k1[i]));
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k2, tr);
 #pragma unroll
     for (int i = 0; i < NV; ++i)
-      ys[i] = ry.y[i] + (S)(h * ((K)dp::A30 * k0[i] + (K)dp::A31 * k1[i] + (K)dp::A32 * k2[i]));
+      ys[i] = upd<M>(ry.y[i], h, madd<M>(madd<M>(c(dp::A30) * k0[i], c(dp::A31), k1[i]), c(dp::A32), k2[i]));
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k3, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      ys[i] = ry.y[i] +
-              (S)(h * ((K)dp::A40 * k0[i] + (K)dp::A41 * k1[i] + (K)dp::A42 * k2[i] + (K)dp::A43 * k3[i]));
+    for (int i = 0; i < NV; ++i) {
+      K acc = madd<M>(c(dp::A40) * k0[i], c(dp::A41), k1[i]);
+      acc = madd<M>(madd<M>(acc, c(dp::A42), k2[i]), c(dp::A43), k3[i]);
+      ys[i] = upd<M>(ry.y[i], h, acc);
+    }
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k4, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      ys[i] = ry.y[i] + (S)(h * ((K)dp::A50 * k0[i] + (K)dp::A51 * k1[i] + (K)dp::A52 * k2[i] +
-                                 (K)dp::A53 * k3[i] + (K)dp::A54 * k4[i]));
+    for (int i = 0; i < NV; ++i) {
+      K acc = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
+      acc = madd<M>(madd<M>(madd<M>(acc, c(dp::A52), k2[i]), c(dp::A53), k3[i]), c(dp::A54), k4[i]);
+      ys[i] = upd<M>(ry.y[i], h, acc);
+    }
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k5, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      yn[i] = ry.y[i] + (S)(h * ((K)dp::B0 * k0[i] + (K)dp::B2 * k2[i] + (K)dp::B3 * k3[i] + (K)dp::B4 * k4[i] +
-                                 (K)dp::B5 * k5[i]));
+    for (int i = 0; i < NV; ++i) {
+      K acc = madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]);
+      acc = madd<M>(madd<M>(madd<M>(acc, c(dp::B3), k3[i]), c(dp::B4), k4[i]), c(dp::B5), k5[i]);
+      yn[i] = upd<M>(ry.y[i], h, acc);
+    }
     M::rhs(P, yn[CR], yn[CTH], ry.pt, yn[CPR], yn[CPTH], ry.pph, k6, tr);
   } else {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)0.5 * k0[i]));
+    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(0.5) * k0[i]);
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k1, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)0.5 * k1[i]));
+    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(0.5) * k1[i]);
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k2, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = ry.y[i] + (S)(h * ((K)1.0 * k2[i]));
+    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(1.0) * k2[i]);
     M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k3, tr);
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      yn[i] = ry.y[i] + (S)(h * ((K)dp::RK4_B0 * k0[i] + (K)dp::RK4_B1 * k1[i] + (K)dp::RK4_B2 * k2[i] +
-                                 (K)dp::RK4_B3 * k3[i]));
+    for (int i = 0; i < NV; ++i) {
+      K acc = madd<M>(madd<M>(madd<M>(c(dp::RK4_B0) * k0[i], c(dp::RK4_B1), k1[i]), c(dp::RK4_B2), k2[i]),
+                      c(dp::RK4_B3), k3[i]);
+      yn[i] = upd<M>(ry.y[i], h, acc);
+    }
     M::rhs(P, yn[CR], yn[CTH], ry.pt, yn[CPR], yn[CPTH], ry.pph, k6, tr);
   }
   bool finite = true;
@@ -513,9 +548,11 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
       N q[NV];
 #pragma unroll
       for (int i = 0; i < NV; ++i) {
-        const K e = h * ((K)dp::E0 * k0[i] + (K)dp::E2 * k2[i] + (K)dp::E3 * k3[i] + (K)dp::E4 * k4[i] +
-                         (K)dp::E5 * k5[i] + (K)dp::E6 * k6[i]);
-        const N scale = (N)P.atol + (N)P.rtol * py_max((N)fabs(ry.y[i]), (N)fabs(yn[i]));
+        K esum = madd<M>(c(dp::E0) * k0[i], c(dp::E2), k2[i]);
+        esum = madd<M>(madd<M>(madd<M>(madd<M>(esum, c(dp::E3), k3[i]), c(dp::E4), k4[i]), c(dp::E5), k5[i]),
+                       c(dp::E6), k6[i]);
+        const K e = h * esum;
+        const N scale = madd<M>((N)P.atol, (N)P.rtol, py_max((N)fabs(ry.y[i]), (N)fabs(yn[i])));
         const N v = (N)e / scale;
         q[i] = v * v;
       }

@@ -1,4 +1,6 @@
-// Kernels with FMA contraction: FP64 (Fast64) and FP32 stages with FP64 accumulation (Mixed).
+// Fast kernels: FP64 (Fast64) and FP32 stages with FP64 accumulation (Mixed).  Their FMAs are
+// written out in the source; the translation unit is compiled with -fmad=false so the compiler
+// fuses nothing else and every launch variant (register cap) computes identical results.
 #include "krr_launch.h"
 
 namespace krr {

@@ -35,6 +35,7 @@ struct Queue {
   unsigned long long busy_iters;  // lane slots that advanced a running photon
   int error;                      // KRR error code raised on the device, or 0
   int pad;
+  unsigned long long flagged;     // photons appended to the re-trace list
 };
 
 // Initial state of global photon g: a row of Y0, or the camera pixel of its image.
@@ -100,11 +101,16 @@ __global__ void k_trace_plain(Params P, const Image* __restrict__ images, int n_
 
 // MAXT threads per block and MINB resident blocks per SM are the launch bounds: the register
 // cap (65536 / (MAXT * MINB)) that trades per-thread registers against resident warps.
+// Queue entries are global photon indices, or positions in `index` (a re-trace list) when it
+// is given; the number of entries is `total`, or *d_total when that is given (a count written
+// on the device by the kernel before, so the launch can sit in a captured graph).
 template <class M, bool RK4, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_trace_persistent(const Image* __restrict__ images, int n_images, long long total,
-                       const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q, int refill_threshold) {
+                       const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q, int refill_threshold,
+                       const long long* __restrict__ index, const unsigned long long* __restrict__ d_total) {
   constexpr unsigned FULL = 0xffffffffu;
+  if (d_total) total = (long long)*d_total;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   Ray<M> ry;
@@ -126,7 +132,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
       if (!active) {
         const unsigned long long mine = base + (unsigned long long)__popc(idle & lt_mask);
         if (mine < (unsigned long long)total) {
-          g = (long long)mine;
+          g = index ? index[mine] : (long long)mine;
           img = find_image(images, n_images, g);
           const Image& im = images[img];
           double y0[8];
@@ -178,6 +184,13 @@ __global__ void __launch_bounds__(MAXT, MINB)
   }
 }
 
+// Flag the pixels whose classification the FP64 re-trace must settle: every photon that did not
+// end ESCAPED or CAPTURED, and every pixel with a different code from one of its 8 neighbours
+// in the same image (the shadow edge).  Flagged global indices are appended to `list` (at most
+// `total` entries; each photon once) and counted in q->flagged.
+__global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, long long total,
+                                const long long* __restrict__ state, long long* __restrict__ list, Queue* q);
+
 // ------------------------------------------------------------------------------------------
 // Launch helpers shared by the two translation units.
 // ------------------------------------------------------------------------------------------
@@ -202,6 +215,8 @@ struct PersistArgs {
   int refill_threshold;
   int grid;
   int block;
+  const long long* index;             // re-trace list (nullable)
+  const unsigned long long* d_total;  // device-side entry count (nullable)
 };
 
 template <class M, bool RK4>
@@ -214,9 +229,9 @@ cudaError_t run_plain(const PlainArgs& a, int block, cudaStream_t s) {
 
 template <class M, bool RK4, int MAXT, int MINB>
 cudaError_t run_persistent(const PersistArgs& a, cudaStream_t s) {
-  if (a.total <= 0) return cudaSuccess;
+  if (a.total <= 0 && !a.d_total) return cudaSuccess;
   k_trace_persistent<M, RK4, MAXT, MINB><<<a.grid, MAXT, 0, s>>>(a.images, a.n_images, a.total, a.Y0, a.o, a.q,
-                                                                  a.refill_threshold);
+                                                                  a.refill_threshold, a.index, a.d_total);
   return cudaGetLastError();
 }
 

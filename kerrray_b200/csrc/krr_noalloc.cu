@@ -59,7 +59,8 @@ extern "C" int krr_trace_images_noalloc(int device, const krr_image* images, int
     return fail(KRR_ERR_INVALID, "krr_trace_images_noalloc takes at most %d images (got %d); use krr_trace_images_device",
                 KRR_NOALLOC_MAX_IMAGES, n_images);
   if (!d_out || !d_out->Y || !d_out->state) return fail(KRR_ERR_INVALID, "Y and state must not be NULL");
-  if (launch && launch->plain) return fail(KRR_ERR_UNSUPPORTED, "krr_trace_images_noalloc runs the persistent kernel only");
+  if (launch && (launch->plain || launch->retrace))
+    return fail(KRR_ERR_UNSUPPORTED, "krr_trace_images_noalloc runs the persistent kernel only, without the re-trace");
   const int32_t precision = launch ? launch->precision : KRR_PREC_FAST64;
   // Descriptors are built in a fixed host buffer: no heap allocation either.
   krr::Image ims[KRR_NOALLOC_MAX_IMAGES];
@@ -124,6 +125,9 @@ extern "C" int krr_trace_images_noalloc(int device, const krr_image* images, int
     stats->lane_slots = q.lane_iters;
     stats->busy_slots = q.busy_iters;
     stats->kernel_ms = 0.0;
+    stats->retraced = 0;
+    stats->retrace_attempts = 0;
+    stats->retrace_ms = 0.0;
   }
   if (q.error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
   if (q.retired != (unsigned long long)total)

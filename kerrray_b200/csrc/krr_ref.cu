@@ -20,6 +20,45 @@ const Variant* ref_variants(bool dtype32, bool rk4, int* count) {
   return rk4 ? v64rk4 : v64;
 }
 
+__global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, long long total,
+                                const long long* __restrict__ state, long long* __restrict__ list, Queue* q) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  bool flag = false;
+  if (g < total) {
+    const Image& im = images[find_image(images, n_images, g)];
+    const long long n = im.res;
+    const long long p = g - im.offset;
+    const long long i = p / n, j = p - (p / n) * n;
+    const long long s = state[g];
+    flag = !(s == ESCAPED || s == CAPTURED);
+    for (int di = -1; di <= 1 && !flag; ++di) {
+      for (int dj = -1; dj <= 1 && !flag; ++dj) {
+        const long long ii = i + di, jj = j + dj;
+        if ((di == 0 && dj == 0) || ii < 0 || ii >= n || jj < 0 || jj >= n) continue;
+        flag = state[im.offset + ii * n + jj] != s;
+      }
+    }
+  }
+  const unsigned mask = __ballot_sync(FULL, flag);
+  if (mask) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if ((int)lane == leader) base = atomicAdd(&q->flagged, (unsigned long long)__popc(mask));
+    base = __shfl_sync(FULL, base, leader);
+    if (flag) list[base + __popc(mask & ((1u << lane) - 1u))] = g;
+  }
+}
+
+cudaError_t flag_boundary(const Image* images, int n_images, long long total, const long long* state, long long* list,
+                          Queue* q, cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  const int block = 256;  // a multiple of 32: the append is warp-aggregated
+  k_flag_boundary<<<(unsigned)((total + block - 1) / block), block, 0, s>>>(images, n_images, total, state, list, q);
+  return cudaGetLastError();
+}
+
 // Camera kernel: one image point per thread.
 __global__ void k_camera_states(Frame F, double fov, long long res, const double* __restrict__ alpha,
                                 const double* __restrict__ beta, long long n, double* __restrict__ Y0, int* err) {

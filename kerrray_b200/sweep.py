@@ -57,6 +57,7 @@ class LaunchConfig:
     refill_threshold: int = 0  # idle lanes before a warp refills (0 = 1)
     plain: bool = False       # one thread per photon instead of the work queue
     variant: int = 0          # compiled launch shape of the persistent kernel
+    retrace: bool = False     # re-trace edge and failed pixels with the reference-order FP64 kernel
 
 
 def order_by_cost(specs: Sequence[ImageSpec]) -> list[int]:
@@ -81,7 +82,8 @@ def _launch(precision: str, cfg: LaunchConfig | None) -> _lib.KrrLaunch:
         raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}, got {precision!r}")
     cfg = cfg or LaunchConfig()
     return _lib.KrrLaunch(precision=_lib.PRECISIONS[precision], block=cfg.block, blocks_per_sm=cfg.blocks_per_sm,
-                          refill_threshold=cfg.refill_threshold, plain=int(cfg.plain), variant=cfg.variant)
+                          refill_threshold=cfg.refill_threshold, plain=int(cfg.plain), variant=cfg.variant,
+                          retrace=int(cfg.retrace), reserved=0)
 
 
 @dataclass
@@ -164,20 +166,23 @@ def trace_images(specs: Sequence[ImageSpec], *, precision: str = "fast64", launc
 class DeviceSweep:
     """A batched launch whose results stay in device memory (torch tensors on ``cuda:device``).
 
-    Build once, then call :meth:`run` repeatedly; each run re-traces every image on the
-    current torch stream and returns the launch statistics (``kernel_ms`` measured with CUDA
-    events on that stream).
+    Build once, then call :meth:`run` repeatedly on the current torch stream. With
+    ``graph=True`` (default) the whole launch sequence is captured once as a CUDA graph
+    (``krr_plan_create``) and each run replays it; ``run(stats=False)`` only enqueues. With
+    ``graph=False`` each run goes through ``krr_trace_images_device`` and reports the trace
+    kernel's CUDA-event time (``kernel_ms``).
     """
 
     def __init__(self, specs: Sequence[ImageSpec], *, precision: str = "fast64", launch: LaunchConfig | None = None,
-                 device: int = 0, Y0=None, minimal: bool = False) -> None:
+                 device: int = 0, Y0=None, minimal: bool = False, graph: bool = True) -> None:
         import torch
 
         self.specs = list(specs)
         self.images, self.offsets = _images(self.specs)
         self.total = int(self.offsets[-1])
         self.device = device
-        self.launch = _launch(precision, launch)
+        self.config = launch or LaunchConfig()
+        self.launch = _launch(precision, self.config)
         dev = torch.device("cuda", device)
         n = self.total
         f64, i64 = torch.float64, torch.int64
@@ -188,18 +193,54 @@ class DeviceSweep:
             for name in ("lam", "max_null_error", "max_energy_drift", "max_lz_drift", "max_carter_drift"):
                 self.tensors[name] = torch.empty(n, dtype=f64, device=dev)
         self.Y0 = Y0
-        ws = int(_lib.lib().krr_workspace_size(len(self.specs)))
+        ws = int(_lib.lib().krr_workspace_size(len(self.specs), n if self.config.retrace else 0))
         self.workspace = torch.zeros(max(ws, 256), dtype=torch.uint8, device=dev)
         self._res = _lib.result_struct(self.tensors, device=True)
+        self.plan = None
+        if graph:
+            handle = ctypes.c_void_p()
+            y0 = None if self.Y0 is None else self.Y0.data_ptr()
+            _lib.check(_lib.lib().krr_plan_create(device, self.images, len(self.specs), y0, ctypes.byref(self.launch),
+                                                  ctypes.byref(self._res), self.workspace.data_ptr(),
+                                                  self.workspace.numel(), ctypes.byref(handle)))
+            self.plan = handle
 
-    def run(self) -> dict[str, Any]:
+    def run(self, stats: bool = True) -> dict[str, Any] | None:
         import torch
 
-        stats = _lib.KrrStats()
         stream = torch.cuda.current_stream(self.device).cuda_stream
+        st = _lib.KrrStats()
+        if self.plan is not None:
+            _lib.check(_lib.lib().krr_plan_launch(self.plan, stream))
+            if not stats:
+                return None
+            _lib.check(_lib.lib().krr_plan_stats(self.plan, stream, ctypes.byref(st)))
+            return st.as_dict()
         y0 = None if self.Y0 is None else self.Y0.data_ptr()
         rc = _lib.lib().krr_trace_images_device(self.device, self.images, len(self.specs), y0, ctypes.byref(self.launch),
-                                                ctypes.byref(self._res), self.workspace.data_ptr(), stream,
-                                                ctypes.byref(stats))
+                                                ctypes.byref(self._res), self.workspace.data_ptr(),
+                                                self.workspace.numel(), stream, ctypes.byref(st))
         _lib.check(rc)
-        return stats.as_dict()
+        return st.as_dict()
+
+    def stats(self) -> dict[str, Any]:
+        """Counters of the last graph launch (synchronises the current stream)."""
+        import torch
+
+        if self.plan is None:
+            raise RuntimeError("stats() reads a captured plan; build the sweep with graph=True")
+        st = _lib.KrrStats()
+        _lib.check(_lib.lib().krr_plan_stats(self.plan, torch.cuda.current_stream(self.device).cuda_stream,
+                                             ctypes.byref(st)))
+        return st.as_dict()
+
+    def close(self) -> None:
+        if self.plan is not None:
+            _lib.lib().krr_plan_destroy(self.plan)
+            self.plan = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

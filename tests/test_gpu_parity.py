@@ -255,3 +255,45 @@ def test_autotuner_picks_a_measured_candidate() -> None:
     cfg, report = K.autotune(specs, precision="fast64", use_cache=False, thresholds=(1, 8), repeats=1)
     assert report["trials"] and report["ms"] == min(t["ms"] for t in report["trials"])
     assert (cfg.variant, cfg.refill_threshold) in {(t["variant"], t["refill_threshold"]) for t in report["trials"]}
+
+
+def _spin99_specs(res: int):
+    cam = K.Camera(radius=1000.0, inclination_deg=85.0, fov=8.0, resolution=res)
+    return [K.ImageSpec(K.Spacetime(1.0, 0.99), cam, K.IntegratorOptions(rtol=1e-6, atol=1e-8), K.TerminationOptions()),
+            K.ImageSpec(K.Spacetime(1.0, 0.5), K.Camera(radius=1000.0, inclination_deg=17.0, fov=8.0, resolution=res // 2),
+                        K.IntegratorOptions(rtol=1e-6, atol=1e-8), K.TerminationOptions())]
+
+
+def test_mixed_with_fp64_retrace_reproduces_the_plain_fp64_mask() -> None:
+    """FP32 stages + FP64 re-trace of edge/failed pixels: the mask of the plain FP64 kernel, exactly."""
+    specs = _spin99_specs(256)
+    plain = K.trace_images(specs, precision="reference", launch=K.LaunchConfig(plain=True))
+    mixed = K.trace_images(specs, precision="mixed", launch=K.LaunchConfig(retrace=True))
+    assert mixed.stats["retraced"] > 0 and mixed.stats["retired"] == mixed.stats["photons"]
+    assert np.array_equal(mixed.arrays["state"], plain.arrays["state"])
+    # The re-traced pixels carry exactly the plain kernel's FP64 results.
+    raw = K.trace_images(specs, precision="mixed")
+    changed = np.flatnonzero(np.any(raw.arrays["Y"] != mixed.arrays["Y"], axis=1))
+    assert changed.size > 0
+    assert np.array_equal(mixed.arrays["Y"][changed], plain.arrays["Y"][changed])
+    # Without the re-trace, any difference from FP64 sits on the edge (re-traced above).
+    esc = (plain.arrays["state"] == 1) & (mixed.arrays["state"] == 1)
+    rel = np.max(_rel(mixed.arrays["Y"][esc], plain.arrays["Y"][esc]), axis=1)
+    print(f"mixed vs plain FP64: {mixed.stats['retraced']} re-traced, escaped max rel dY {rel.max():.2e}, "
+          f"median {np.median(rel):.2e}")
+
+
+def test_captured_graph_plan_equals_direct_launch() -> None:
+    torch = pytest.importorskip("torch")
+    specs = _spin99_specs(128)
+    for precision, retrace in (("fast64", False), ("mixed", True), ("reference", False)):
+        cfg = K.LaunchConfig(retrace=retrace)
+        direct = K.trace_images(specs, precision=precision, launch=cfg)
+        sw = K.DeviceSweep(specs, precision=precision, launch=cfg, graph=True)
+        for _ in range(2):  # replays reset the counters
+            st = sw.run()
+            assert st["retired"] == st["photons"] == direct.stats["photons"]
+            assert st["attempts"] == direct.stats["attempts"] and st.get("retraced") == direct.stats["retraced"]
+            assert np.array_equal(sw.tensors["Y"].cpu().numpy(), direct.arrays["Y"])
+            assert np.array_equal(sw.tensors["state"].cpu().numpy(), direct.arrays["state"])
+        sw.close()
