@@ -69,9 +69,13 @@ struct Params {
   double mass, a, a2, neg_2ma, pos_2ma, two_m, two_a2;
   double rtol, atol, h0, h_min, h_max, lambda_max;
   double r_capture, r_escape, r_in, r_out;
+  double r_plus;  // outer horizon M + sqrt(M^2 - a^2)
   long long max_steps, guard;
   int rk4;   // 0: Dormand-Prince 5(4), 1: fixed-step RK4
   int disk;  // disk-plane event enabled
+  // FP32 copies for the mixed mode's stages (rounded once on the host).
+  float f_mass, f_a2, f_neg_2ma, f_pos_2ma, f_two_a2;
+  float f_rpm;  // r_plus - r_minus = 2 sqrt(M^2 - a^2)
 };
 
 // Per-ray conservation references (numba_backend.py:174-178).  E and L_z are exact constants
@@ -91,6 +95,27 @@ __device__ __forceinline__ X py_min(X a, X b) { return (b < a) ? b : a; }  // Py
 __device__ __forceinline__ bool finite_(double x) { return isfinite(x); }
 __device__ __forceinline__ bool finite_(float x) { return isfinite(x); }
 
+// a*x + acc: one fused operation in the fast modes, two roundings (the reference's order) in
+// the reference modes.  Contraction is never left to the compiler, so every launch variant of
+// a mode computes the same bits.
+__device__ __forceinline__ double fused(double a, double x, double acc) { return fma(a, x, acc); }
+__device__ __forceinline__ float fused(float a, float x, float acc) { return fmaf(a, x, acc); }
+
+template <class M, class X>
+__device__ __forceinline__ X madd(X acc, X a, X x) {
+  if constexpr (M::kFused) return fused(a, x, acc);
+  else return acc + a * x;
+}
+
+// y + h * acc, the state update of a stage.  The mixed mode forms h * acc exactly in FP64 (a
+// product of two floats) and rounds once when adding it to the FP64 state.
+template <class M>
+__device__ __forceinline__ typename M::S upd(typename M::S y, typename M::K h, typename M::K acc) {
+  using S = typename M::S;
+  if constexpr (!M::kFused) return y + (S)(h * acc);
+  else return fused((S)h, (S)acc, y);
+}
+
 // Sine and cosine of the last right-hand-side evaluation, reused by classification and the
 // Carter constant (same function, same argument, so the same values the reference recomputes).
 struct Trig {
@@ -108,6 +133,26 @@ struct RefMode {
   static constexpr bool kFused = false;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
+
+  struct Shadow {};
+
+  __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow&, K f[NV], Trig& tr) {
+    rhs(P, y[CR], y[CTH], pt, y[CPR], y[CPTH], pph, f, tr);
+  }
+  __device__ static void accepted(const Params&, const S[NV], Shadow&) {}
+
+  // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state).
+  template <bool LAST, class R>
+  __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
+    S ys[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = upd<RefMode<W>>(ry.y[i], h, acc[i]);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) yn[i] = ys[i];
+    }
+    rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, f, tr);
+  }
 
   __device__ static void metric(const Params& P, double r, double th, double g[15], Trig& tr) {
     const double m = P.mass, a2 = P.a2;
@@ -183,6 +228,26 @@ struct Fast64 {
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
 
+  struct Shadow {};
+
+  __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow&, K f[NV], Trig& tr) {
+    rhs(P, y[CR], y[CTH], pt, y[CPR], y[CPTH], pph, f, tr);
+  }
+  __device__ static void accepted(const Params&, const S[NV], Shadow&) {}
+
+  // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state).
+  template <bool LAST, class R>
+  __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
+    S ys[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ys[i] = upd<Fast64>(ry.y[i], h, acc[i]);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) yn[i] = ys[i];
+    }
+    rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, f, tr);
+  }
+
   __device__ static void rhs(const Params& P, double r, double th, double pt, double pr, double pth, double pph,
                              double f[NV], Trig& tr) {
     const double m = P.mass, a2 = P.a2;
@@ -239,13 +304,21 @@ struct Fast64 {
   }
 };
 
-// FP32 stages with FP64 state accumulation, FP64 Delta and FP64 error norm.
+// FP32 stages from an FP32 shadow of the FP64 state; FP64 state accumulation, error norm,
+// classification and diagnostics.  Delta is formed as (r - r_plus)(r - r_minus): r - r_plus is
+// taken from the FP64 state once per accepted step and carried in FP32, so Delta keeps its
+// relative accuracy down to the capture margin (the quadratic r^2 - 2Mr + a^2 cancels there).
 struct Mixed {
   using S = double;
   using K = float;
   using N = double;
   static constexpr bool kFastFactor = true;
   static constexpr bool kFused = true;
+
+  // FP32 copy of what the stages read: r - r_plus, r, theta, p_r, p_theta and the constants.
+  struct Shadow {
+    float d0, r, th, pr, pth, pt, pph;
+  };
 
   // The accepted state's diagnostics (Carter constant, axis test) use FP64 sine and cosine.
   __device__ static Trig accept_trig(double th, const Trig&) {
@@ -254,25 +327,49 @@ struct Mixed {
     return t;
   }
 
-  __device__ static void rhs(const Params& P, double r, double th, double pt_d, double pr_d, double pth_d,
-                             double pph_d, float f[NV], Trig& tr) {
-    // Delta near the horizon cancels to ~1e-6 of r^2: evaluate it in FP64 before the cast.
-    const float dlt = (float)fma(r, r - P.two_m, P.a2);
-    const float rf = (float)r, thf = (float)th;
-    const float m = (float)P.mass, a2 = (float)P.a2;
+  __device__ static void accepted(const Params& P, const S y[NV], Shadow& sh) {
+    sh.d0 = (float)(y[CR] - P.r_plus);
+    sh.r = (float)y[CR];
+    sh.th = (float)y[CTH];
+    sh.pr = (float)y[CPR];
+    sh.pth = (float)y[CPTH];
+  }
+
+  __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow& sh, K f[NV], Trig& tr) {
+    sh.pt = (float)pt;
+    sh.pph = (float)pph;
+    accepted(P, y, sh);
+    rhs_f(P, sh.d0, sh.r, sh.th, sh.pt, sh.pr, sh.pth, sh.pph, f, tr);
+  }
+
+  template <bool LAST, class R>
+  __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
+    if constexpr (LAST) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) yn[i] = ry.y[i] + (double)(h * acc[i]);  // FP64 accumulation
+    }
+    const Shadow& sh = ry.sh;
+    rhs_f(P, fmaf(h, acc[CR], sh.d0), fmaf(h, acc[CR], sh.r), fmaf(h, acc[CTH], sh.th), sh.pt,
+          fmaf(h, acc[CPR], sh.pr), fmaf(h, acc[CPTH], sh.pth), sh.pph, f, tr);
+  }
+
+  // The right-hand side in FP32 at (r - r_plus = d, r, theta, p).
+  __device__ static void rhs_f(const Params& P, float d, float rf, float thf, float pt, float pr, float pth,
+                               float pph, float f[NV], Trig& tr) {
+    const float dlt = d * (d + P.f_rpm);
+    const float m = P.f_mass, a2 = P.f_a2;
     float s, c;
     sincosf(thf, &s, &c);
     tr.s = (double)s;
     tr.c = (double)c;
-    const float pt = (float)pt_d, pr = (float)pr_d, pth = (float)pth_d, pph = (float)pph_d;
     const float s2 = s * s;
     const float sin2th = 2.0f * s * c;
     const float r2 = rf * rf;
     const float sig = fmaf(a2, c * c, r2);
     const float r2a2 = r2 + a2;
     const float big_a = fmaf(r2a2, r2a2, -a2 * dlt * s2);
-    const float isig = 1.0f / sig;
-    const float idlt = 1.0f / dlt;
+    const float isig = __fdividef(1.0f, sig);
+    const float idlt = __fdividef(1.0f, dlt);
     const float isd = isig * idlt;
     const float isd2 = isd * isd;
     const float isig2 = isig * isig;
@@ -280,26 +377,25 @@ struct Mixed {
     const float sig_r = 2.0f * rf;
     const float sig_th = -a2 * sin2th;
     const float dlt_r = 2.0f * (rf - m);
-    const float a_r = fmaf(4.0f * rf, r2a2, -(float)P.two_a2 * (rf - m) * s2);
+    const float a_r = fmaf(4.0f * rf, r2a2, -P.f_two_a2 * (rf - m) * s2);
     const float a_th = -a2 * dlt * sin2th;
     const float sd_r = fmaf(sig_r, dlt, sig * dlt_r);
     const float sd_th = sig_th * dlt;
-    const float neg_2ma = (float)P.neg_2ma, pos_2ma = (float)P.pos_2ma;
     const float g0 = -big_a * isd;
-    const float g1 = neg_2ma * rf * isd;
+    const float g1 = P.f_neg_2ma * rf * isd;
     const float g2 = dlt * isig;
     const float g3 = isig;
     const float g5 = fmaf(big_a, sd_r, -a_r * sd) * isd2;
-    const float g6 = neg_2ma * fmaf(-rf, sd_r, sd) * isd2;
+    const float g6 = P.f_neg_2ma * fmaf(-rf, sd_r, sd) * isd2;
     const float g7 = fmaf(dlt_r, sig, -dlt * sig_r) * isig2;
     const float g8 = -sig_r * isig2;
     const float g10 = fmaf(big_a, sd_th, -a_th * sd) * isd2;
-    const float g11 = pos_2ma * rf * sd_th * isd2;
+    const float g11 = P.f_pos_2ma * rf * sd_th * isd2;
     const float g12 = -dlt * sig_th * isig2;
     const float g13 = -sig_th * isig2;
     float g4 = 0.0f, g9 = 0.0f, g14 = 0.0f;
-    if (pph_d != 0.0) {
-      const float is2 = 1.0f / s2;
+    if (pph != 0.0f) {  // polar-axis guard
+      const float is2 = __fdividef(1.0f, s2);
       g4 = fmaf(-a2, s2, dlt) * isd * is2;
       g9 = fmaf(-sig_r * isig2, is2, a2 * sd_r * isd2);
       g14 = fmaf(-fmaf(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
@@ -329,6 +425,7 @@ struct Ray {
   double m_null, m_q;
   Refs ref;
   Trig tr;   // sin/cos of theta at y
+  typename M::Shadow sh;
   long long attempts;
   int n_steps, n_rej;
   int state;
@@ -401,7 +498,7 @@ __device__ __forceinline__ void ray_init(const Params& P, const double y0[8], do
   ry.ref.q0 = q0;
   ry.ref.fq = fe * fe * P.mass * P.mass;
   ry.ref.fe2 = fe * fe;
-  M::rhs(P, ry.y[CR], ry.y[CTH], ry.pt, ry.y[CPR], ry.y[CPTH], ry.pph, ry.f, ry.tr);
+  M::init_rhs(P, ry.y, ry.pt, ry.pph, ry.sh, ry.f, ry.tr);
   ry.m_null = null_error<M>(ry) / ry.ref.fe2;
   ry.m_q = 0.0;
   ry.lam = 0.0;
@@ -441,27 +538,6 @@ __device__ __forceinline__ typename M::N step_factor(typename M::N en, bool reje
   return factor;
 }
 
-// a*x + acc: one fused operation in the fast modes, two roundings (the reference's order) in
-// the reference modes.  Contraction is never left to the compiler, so every launch variant of
-// a mode computes the same bits.
-__device__ __forceinline__ double fused(double a, double x, double acc) { return fma(a, x, acc); }
-__device__ __forceinline__ float fused(float a, float x, float acc) { return fmaf(a, x, acc); }
-
-template <class M, class X>
-__device__ __forceinline__ X madd(X acc, X a, X x) {
-  if constexpr (M::kFused) return fused(a, x, acc);
-  else return acc + a * x;
-}
-
-// y + h * acc, the state update of a stage.  The mixed mode forms h * acc exactly in FP64 (a
-// product of two floats) and rounds once when adding it to the FP64 state.
-template <class M>
-__device__ __forceinline__ typename M::S upd(typename M::S y, typename M::K h, typename M::K acc) {
-  using S = typename M::S;
-  if constexpr (!M::kFused) return y + (S)(h * acc);
-  else return fused((S)h, (S)acc, y);
-}
-
 // One step attempt (numba_kernel.py:376-455): DP5(4) (or RK4) step, error norm, controller,
 // accept/reject, diagnostics and classification.  Returns with ry.state updated.
 template <class M, bool RK4>
@@ -480,61 +556,56 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   const S h_eff = last ? (S)remaining : ry.h;
   const K h = (K)h_eff;
   K k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV];
-  S ys[NV], yn[NV];
+  S yn[NV];
   Trig tr;
   const K* k0 = ry.f;
   // Stage inputs: the reference's sums (same terms and order, zero coefficients skipped);
-  // madd / upd fuse them in the fast modes and round each operation in the reference modes.
+  // madd fuses them in the fast modes and rounds each operation in the reference modes.
   auto c = [](double x) { return (K)x; };
+  K acc[NV];
   if constexpr (!RK4) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(dp::A10) * k0[i]);
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k1, tr);
+    for (int i = 0; i < NV; ++i) acc[i] = c(dp::A10) * k0[i];
+    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, madd<M>(c(dp::A20) * k0[i], c(dp::A21), k1[i]));
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k2, tr);
+    for (int i = 0; i < NV; ++i) acc[i] = madd<M>(c(dp::A20) * k0[i], c(dp::A21), k1[i]);
+    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      ys[i] = upd<M>(ry.y[i], h, madd<M>(madd<M>(c(dp::A30) * k0[i], c(dp::A31), k1[i]), c(dp::A32), k2[i]));
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k3, tr);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      K acc = madd<M>(c(dp::A40) * k0[i], c(dp::A41), k1[i]);
-      acc = madd<M>(madd<M>(acc, c(dp::A42), k2[i]), c(dp::A43), k3[i]);
-      ys[i] = upd<M>(ry.y[i], h, acc);
-    }
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k4, tr);
+    for (int i = 0; i < NV; ++i) acc[i] = madd<M>(madd<M>(c(dp::A30) * k0[i], c(dp::A31), k1[i]), c(dp::A32), k2[i]);
+    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
-      K acc = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
-      acc = madd<M>(madd<M>(madd<M>(acc, c(dp::A52), k2[i]), c(dp::A53), k3[i]), c(dp::A54), k4[i]);
-      ys[i] = upd<M>(ry.y[i], h, acc);
+      const K a = madd<M>(c(dp::A40) * k0[i], c(dp::A41), k1[i]);
+      acc[i] = madd<M>(madd<M>(a, c(dp::A42), k2[i]), c(dp::A43), k3[i]);
     }
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k5, tr);
+    M::template stage<false>(P, ry, h, acc, k4, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
-      K acc = madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]);
-      acc = madd<M>(madd<M>(madd<M>(acc, c(dp::B3), k3[i]), c(dp::B4), k4[i]), c(dp::B5), k5[i]);
-      yn[i] = upd<M>(ry.y[i], h, acc);
+      const K a = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
+      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::A52), k2[i]), c(dp::A53), k3[i]), c(dp::A54), k4[i]);
     }
-    M::rhs(P, yn[CR], yn[CTH], ry.pt, yn[CPR], yn[CPTH], ry.pph, k6, tr);
+    M::template stage<false>(P, ry, h, acc, k5, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      const K a = madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]);
+      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::B3), k3[i]), c(dp::B4), k4[i]), c(dp::B5), k5[i]);
+    }
+    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
   } else {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(0.5) * k0[i]);
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k1, tr);
+    for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k0[i];
+    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(0.5) * k1[i]);
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k2, tr);
+    for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k1[i];
+    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) ys[i] = upd<M>(ry.y[i], h, c(1.0) * k2[i]);
-    M::rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, k3, tr);
+    for (int i = 0; i < NV; ++i) acc[i] = c(1.0) * k2[i];
+    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      K acc = madd<M>(madd<M>(madd<M>(c(dp::RK4_B0) * k0[i], c(dp::RK4_B1), k1[i]), c(dp::RK4_B2), k2[i]),
-                      c(dp::RK4_B3), k3[i]);
-      yn[i] = upd<M>(ry.y[i], h, acc);
-    }
-    M::rhs(P, yn[CR], yn[CTH], ry.pt, yn[CPR], yn[CPTH], ry.pph, k6, tr);
+    for (int i = 0; i < NV; ++i)
+      acc[i] = madd<M>(madd<M>(madd<M>(c(dp::RK4_B0) * k0[i], c(dp::RK4_B1), k1[i]), c(dp::RK4_B2), k2[i]),
+                       c(dp::RK4_B3), k3[i]);
+    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
   }
   bool finite = true;
 #pragma unroll
@@ -595,6 +666,7 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
     ry.y[i] = yn[i];
     ry.f[i] = k6[i];
   }
+  M::accepted(P, ry.y, ry.sh);
   ry.tr = M::accept_trig((double)ry.y[CTH], tr);
   const double lam_old = ry.lam;
   ry.lam = last ? P.lambda_max : ry.lam + (double)h_eff;
