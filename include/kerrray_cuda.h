@@ -209,6 +209,27 @@ KRR_API int krr_plan_launch(krr_plan* plan, void* stream);
 KRR_API int krr_plan_stats(krr_plan* plan, void* stream, krr_stats* stats);
 KRR_API int krr_plan_destroy(krr_plan* plan);
 
+/* One case of a batched edge bisection: spacetime, observer, integrator options and the
+ * image-plane centre the polar angles are measured about. */
+typedef struct krr_edge_case {
+  double mass, spin;
+  double radius, inclination_deg, phi_deg;
+  krr_options options;
+  double centre_alpha, centre_beta;
+} krr_edge_case;
+
+/* Bisect the image radius of the shadow edge along n_items polar directions on the device
+ * (scripts/study_edge_bisection.py:53-68, bisect_edge, with its PointCamera :39-50): item k
+ * belongs to case item_case[k], looks along (cos_phi[k], sin_phi[k]) and starts from the
+ * bracket [lo[k], hi[k]] (captured at lo, escaped at hi); each of `iterations` halvings traces
+ * the photon at mid = (lo + hi) / 2 and moves hi to mid if it ESCAPED, lo otherwise.  lo and hi
+ * are updated in place (host arrays); failures[k] (nullable) counts results that were neither
+ * ESCAPED nor CAPTURED.  All iterations of all items run in one persistent launch. */
+KRR_API int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, const int32_t* item_case,
+                             const double* cos_phi, const double* sin_phi, double* lo, double* hi,
+                             int64_t* failures, int64_t n_items, int32_t iterations, int32_t precision,
+                             krr_stats* stats);
+
 /* Allocation-free form of krr_trace_images_device.  No counterpart in the reference.  For
  * callers that cannot allocate device memory on this path (an application that owns a fixed
  * device-memory budget, work enqueued on a stream another library captures, a plug-in whose

@@ -15,7 +15,18 @@ from kerrray_b200.backends import (
     get_backend,
     register_with_kerrray,
 )
+from kerrray_b200.bisect import EdgeCase, bisect_edge, bisect_edges, edge_options, edge_study
+from kerrray_b200.boundary import (
+    analytic_boundary,
+    boundary_error,
+    extract_boundary_from_mask,
+    finite_distance_scale,
+    polygon_centroid,
+    polygon_radii,
+    summarise_shadow,
+)
 from kerrray_b200.camera import Camera, initial_states, initial_states_at
+from kerrray_b200.orbits import critical_impact_parameters, shadow_curve
 from kerrray_b200.rays import concatenate_results, trace_rays
 from kerrray_b200.shadow import FAILURE_STATES, ShadowImage, compute_shadow, shadow_mask_int8, state_counts
 from kerrray_b200.sweep import DeviceSweep, ImageSpec, LaunchConfig, SweepResult, order_by_cost, trace_images
@@ -31,6 +42,9 @@ from kerrray_b200.types import (
 )
 
 __all__ = [
+    "EdgeCase", "analytic_boundary", "bisect_edge", "bisect_edges", "boundary_error", "critical_impact_parameters",
+    "edge_options", "edge_study", "extract_boundary_from_mask", "finite_distance_scale", "polygon_centroid",
+    "polygon_radii", "shadow_curve", "summarise_shadow",
     "BACKEND_NAMES", "Backend", "BackendUnavailable", "BatchResult", "Camera", "CudaBackend", "DeviceSweep",
     "EventOptions", "FAILURE_STATES", "ImageSpec", "IntegratorOptions", "LaunchConfig", "ShadowImage", "Spacetime",
     "SweepResult", "TerminationOptions", "TerminationState", "autotune", "available_backends", "compute_shadow",

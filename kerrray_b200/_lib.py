@@ -26,7 +26,7 @@ EXPORTS = (
     "krr_last_error", "krr_abi_version", "krr_device_count", "krr_max_attempts", "krr_integrate_batch",
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
     "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
-    "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy",
+    "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy", "krr_bisect_edges",
 )
 
 
@@ -59,6 +59,12 @@ class KrrCamera(ctypes.Structure):
 
 class KrrImage(ctypes.Structure):
     _fields_ = [("mass", ctypes.c_double), ("spin", ctypes.c_double), ("camera", KrrCamera), ("options", KrrOptions)]
+
+
+class KrrEdgeCase(ctypes.Structure):
+    _fields_ = [("mass", ctypes.c_double), ("spin", ctypes.c_double), ("radius", ctypes.c_double),
+                ("inclination_deg", ctypes.c_double), ("phi_deg", ctypes.c_double), ("options", KrrOptions),
+                ("centre_alpha", ctypes.c_double), ("centre_beta", ctypes.c_double)]
 
 
 class KrrLaunch(ctypes.Structure):
@@ -124,6 +130,9 @@ def lib() -> ctypes.CDLL:
         L.krr_trace_images_device.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
                                               ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp,
                                               ctypes.c_size_t, vp, ctypes.POINTER(KrrStats)]
+        L.krr_bisect_edges.restype = ctypes.c_int
+        L.krr_bisect_edges.argtypes = [ctypes.c_int, ctypes.POINTER(KrrEdgeCase), i32, vp, vp, vp, vp, vp, vp, i64, i32,
+                                       i32, ctypes.POINTER(KrrStats)]
         L.krr_plan_create.restype = ctypes.c_int
         L.krr_plan_create.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp, ctypes.POINTER(KrrLaunch),
                                       ctypes.POINTER(KrrResult), vp, ctypes.c_size_t, ctypes.POINTER(vp)]

@@ -1,0 +1,120 @@
+"""Shadow-edge bisection on the device.
+
+Restates ``bisect_edge`` of ``scripts/study_edge_bisection.py:53-68`` (with its ``PointCamera``,
+``:39-50``): along each polar direction about an image-plane centre the image radius is halved
+between a captured and an escaped photon; the integrator uses ``rtol``, ``atol = 1e-2 rtol``,
+``max_steps = 2e6``, ``lambda_max = 4 r_o`` and terminates at ``r_o`` with a 1e-6 horizon
+margin. Here every direction of every case is one work item of a single persistent launch
+(``krr_bisect_edges``): a lane runs all the halvings of its item in registers.
+
+:func:`edge_study` builds the reference's study set-up for one case -- the Bardeen curve's
+centroid scaled by the finite-distance factor as centre, a bracket around the curve's radius
+-- and reports the edge error against the curve.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import Any, Sequence
+
+import numpy as np
+
+from kerrray_b200 import _lib
+from kerrray_b200.boundary import analytic_boundary, finite_distance_scale, polygon_centroid, polygon_radii
+from kerrray_b200.types import IntegratorOptions, TerminationOptions
+
+__all__ = ["EdgeCase", "bisect_edge", "bisect_edges", "edge_options", "edge_study"]
+
+
+def edge_options(rtol: float, r_o: float) -> tuple[IntegratorOptions, TerminationOptions]:
+    """The integrator and termination options of the edge study (study_edge_bisection.py:54-55)."""
+    integ = IntegratorOptions(method="rk45", rtol=rtol, atol=rtol * 1e-2, max_steps=2_000_000, lambda_max=4.0 * r_o)
+    return integ, TerminationOptions(horizon_epsilon=1e-6, escape_radius=r_o)
+
+
+@dataclass
+class EdgeCase:
+    """One bisection case: spacetime, observer, tolerance, centre, directions and brackets."""
+
+    spacetime: Any
+    inclination_deg: float
+    r_o: float
+    rtol: float
+    centre: tuple[float, float]
+    angles: np.ndarray
+    r_lo: np.ndarray
+    r_hi: np.ndarray
+
+    def struct(self) -> _lib.KrrEdgeCase:
+        integ, term = edge_options(self.rtol, self.r_o)
+        return _lib.KrrEdgeCase(mass=float(self.spacetime.mass), spin=float(self.spacetime.spin), radius=float(self.r_o),
+                                inclination_deg=float(self.inclination_deg), phi_deg=0.0,
+                                options=_lib.options_struct(integ, term), centre_alpha=float(self.centre[0]),
+                                centre_beta=float(self.centre[1]))
+
+
+def bisect_edges(cases: Sequence[EdgeCase], iterations: int, *, precision: str = "reference",
+                 device: int = 0) -> tuple[list[tuple[np.ndarray, np.ndarray, int]], dict]:
+    """Run every case's bisection in one launch; per case ``(r_mid, width, failures)`` and the stats."""
+    cases = list(cases)
+    arr = (_lib.KrrEdgeCase * len(cases))(*[c.struct() for c in cases])
+    sizes = [np.asarray(c.angles).size for c in cases]
+    item_case = np.concatenate([np.full(n, k, dtype=np.int32) for k, n in enumerate(sizes)])
+    angles = np.concatenate([np.asarray(c.angles, dtype=np.float64).ravel() for c in cases])
+    cos_phi, sin_phi = np.ascontiguousarray(np.cos(angles)), np.ascontiguousarray(np.sin(angles))
+    lo = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(c.r_lo, np.float64), (n,))
+                                              for c, n in zip(cases, sizes)]))
+    hi = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(c.r_hi, np.float64), (n,))
+                                              for c, n in zip(cases, sizes)]))
+    fails = np.zeros(lo.size, dtype=np.int64)
+    stats = _lib.KrrStats()
+    if precision not in _lib.PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(_lib.PRECISIONS)}, got {precision!r}")
+    rc = _lib.lib().krr_bisect_edges(device, arr, len(cases), item_case.ctypes.data, cos_phi.ctypes.data,
+                                     sin_phi.ctypes.data, lo.ctypes.data, hi.ctypes.data, fails.ctypes.data, lo.size,
+                                     int(iterations), _lib.PRECISIONS[precision], ctypes.byref(stats))
+    _lib.check(rc)
+    out = []
+    start = 0
+    for n in sizes:
+        sl = slice(start, start + n)
+        out.append((0.5 * (lo[sl] + hi[sl]), hi[sl] - lo[sl], int(fails[sl].sum())))
+        start += n
+    return out, stats.as_dict()
+
+
+def bisect_edge(st, incl, r_o, rtol, centre, angles, r_lo, r_hi, iterations, *, precision: str = "reference",
+                device: int = 0) -> tuple[np.ndarray, np.ndarray, int]:
+    """``(r_mid, width, failures)`` for one case; the arguments of study_edge_bisection.bisect_edge."""
+    case = EdgeCase(st, float(incl), float(r_o), float(rtol), (float(centre[0]), float(centre[1])),
+                    np.asarray(angles, dtype=np.float64), np.asarray(r_lo, dtype=np.float64),
+                    np.asarray(r_hi, dtype=np.float64))
+    (res,), _ = bisect_edges([case], iterations, precision=precision, device=device)
+    return res
+
+
+def edge_study(st, incl: float, r_o: float, rtol: float, angles, *, bracket: tuple[float, float] | None = None,
+               rel_bracket: float = 0.02, n_curve: int = 40000) -> EdgeCase:
+    """The study's case: centre = Bardeen centroid / k; bracket ``(1 -+ rel_bracket) r_Bardeen / k``,
+    or the absolute image radii ``bracket`` about that centre."""
+    k = finite_distance_scale(st, r_o)
+    ca, cb = analytic_boundary(st, incl, n_curve)
+    c_ana = polygon_centroid(ca, cb)
+    angles = np.asarray(angles, dtype=np.float64)
+    if bracket is None:
+        r_img = polygon_radii(ca, cb, c_ana, angles) / k
+        lo, hi = (1.0 - rel_bracket) * r_img, (1.0 + rel_bracket) * r_img
+    else:
+        lo, hi = np.full(angles.size, float(bracket[0])), np.full(angles.size, float(bracket[1]))
+    return EdgeCase(st, incl, r_o, rtol, (c_ana[0] / k, c_ana[1] / k), angles, lo, hi)
+
+
+def edge_error(case: EdgeCase, r_mid: np.ndarray, n_curve: int = 40000) -> dict[str, float]:
+    """Edge error against Bardeen's curve after the finite-distance correction (M)."""
+    k = finite_distance_scale(case.spacetime, case.r_o)
+    ca, cb = analytic_boundary(case.spacetime, case.inclination_deg, n_curve)
+    r_ana = polygon_radii(ca, cb, (case.centre[0] * k, case.centre[1] * k), case.angles)
+    err = r_mid * k - r_ana
+    return {"rms_M": float(np.sqrt(np.mean(err**2))), "max_M": float(np.max(np.abs(err))), "mean_M": float(np.mean(err))}

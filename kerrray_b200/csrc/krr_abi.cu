@@ -792,6 +792,109 @@ int krr_plan_destroy(krr_plan* plan) {
   return KRR_OK;
 }
 
+int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, const int32_t* item_case,
+                     const double* cos_phi, const double* sin_phi, double* lo, double* hi, int64_t* failures,
+                     int64_t n_items, int32_t iterations, int32_t precision, krr_stats* stats) {
+  if (!cases || n_cases < 1) return fail(KRR_ERR_INVALID, "need at least one case");
+  if (n_items < 0 || iterations < 0) return fail(KRR_ERR_INVALID, "n_items and iterations must be >= 0");
+  if (n_items > 0 && (!item_case || !cos_phi || !sin_phi || !lo || !hi))
+    return fail(KRR_ERR_INVALID, "item_case, cos_phi, sin_phi, lo and hi must not be NULL");
+  std::vector<krr::EdgeCase> ec(n_cases);
+  for (int k = 0; k < n_cases; ++k) {
+    const krr_edge_case& c = cases[k];
+    int rc = validate_spacetime(c.mass, c.spin);
+    if (!rc) rc = validate_options(&c.options);
+    if (!rc) rc = check_precision(precision, &c.options);
+    if (rc) return rc;
+    if (c.options.method != 0 || c.options.disk_plane)
+      return fail(KRR_ERR_UNSUPPORTED, "the edge bisection integrates with rk45 and no events");
+    krr_camera cam{c.radius, c.inclination_deg, c.phi_deg, 1.0, 2};
+    rc = make_frame(c.mass, c.spin, &cam, ec[k].F);
+    if (rc) return rc;
+    ec[k].P = make_params(c.mass, c.spin, &c.options);
+    ec[k].c_alpha = c.centre_alpha;
+    ec[k].c_beta = c.centre_beta;
+  }
+  for (int64_t i = 0; i < n_items; ++i) {
+    const int c = item_case[i];
+    if (c < 0 || c >= n_cases) return fail(KRR_ERR_INVALID, "item_case[%lld] = %d out of range", (long long)i, c);
+    if (!(std::isfinite(lo[i]) && std::isfinite(hi[i]) && std::isfinite(cos_phi[i]) && std::isfinite(sin_phi[i])))
+      return fail(KRR_ERR_INVALID, "brackets and directions must be finite");
+    // Every bisection point lies between the bracket ends: both must be directions on the sky.
+    const double r2 = cases[c].radius * cases[c].radius;
+    for (double rho : {lo[i], hi[i]}) {
+      const double al = cases[c].centre_alpha + rho * cos_phi[i], be = cases[c].centre_beta + rho * sin_phi[i];
+      if (!((al * al + be * be) / r2 < 1.0))
+        return fail(KRR_ERR_INVALID, "image points with alpha^2 + beta^2 >= radius^2 are not directions on the sky");
+    }
+  }
+  if (n_items == 0) return KRR_OK;
+  Context* ctx = nullptr;
+  int rc = get_context(device, &ctx);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KRR_CUDA(cudaSetDevice(device));
+  const size_t nb8 = (size_t)n_items * 8, nb4 = (size_t)n_items * 4;
+  const size_t bytes = 512 + round256((size_t)n_cases * sizeof(krr::EdgeCase)) + 5 * round256(nb8) + round256(nb4);
+  KRR_CUDA(ctx->buf[B_AB].ensure(bytes));
+  char* base = static_cast<char*>(ctx->buf[B_AB].p);
+  krr::Queue* d_q = reinterpret_cast<krr::Queue*>(base);
+  size_t off = 512;
+  auto take = [&](size_t n) { char* p = base + off; off += round256(n); return p; };
+  auto* d_cases = reinterpret_cast<krr::EdgeCase*>(take((size_t)n_cases * sizeof(krr::EdgeCase)));
+  auto* d_item = reinterpret_cast<int*>(take(nb4));
+  auto* d_cos = reinterpret_cast<double*>(take(nb8));
+  auto* d_sin = reinterpret_cast<double*>(take(nb8));
+  auto* d_lo = reinterpret_cast<double*>(take(nb8));
+  auto* d_hi = reinterpret_cast<double*>(take(nb8));
+  auto* d_fail = reinterpret_cast<long long*>(take(nb8));
+  const cudaStream_t s = ctx->stream;
+  KRR_CUDA(cudaMemsetAsync(d_q, 0, sizeof(krr::Queue), s));
+  KRR_CUDA(cudaMemcpyAsync(d_cases, ec.data(), ec.size() * sizeof(krr::EdgeCase), cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemcpyAsync(d_item, item_case, nb4, cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemcpyAsync(d_cos, cos_phi, nb8, cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemcpyAsync(d_sin, sin_phi, nb8, cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemcpyAsync(d_lo, lo, nb8, cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemcpyAsync(d_hi, hi, nb8, cudaMemcpyHostToDevice, s));
+  krr::EdgeArgs a{};
+  a.cases = d_cases;
+  a.item_case = d_item;
+  a.cos_phi = d_cos;
+  a.sin_phi = d_sin;
+  a.lo = d_lo;
+  a.hi = d_hi;
+  a.failures = d_fail;
+  a.n_items = n_items;
+  a.iterations = iterations;
+  a.q = d_q;
+  a.refill_threshold = 1;
+  KRR_CUDA(cudaEventRecord(ctx->ev0, s));
+  KRR_CUDA(precision == KRR_PREC_REFERENCE ? krr::ref_bisect(a, s) : krr::fast_bisect(precision == KRR_PREC_MIXED, a, s));
+  KRR_CUDA(cudaEventRecord(ctx->ev1, s));
+  krr::Queue q{};
+  KRR_CUDA(cudaMemcpyAsync(&q, d_q, sizeof(q), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaMemcpyAsync(lo, d_lo, nb8, cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaMemcpyAsync(hi, d_hi, nb8, cudaMemcpyDeviceToHost, s));
+  if (failures) KRR_CUDA(cudaMemcpyAsync(failures, d_fail, nb8, cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.0f;
+  KRR_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->photons = (uint64_t)n_items * (uint64_t)iterations;
+    stats->retired = q.retired;
+    stats->attempts = q.attempts;
+    stats->accepted = q.accepted;
+    stats->lane_slots = q.lane_iters;
+    stats->busy_slots = q.busy_iters;
+    stats->kernel_ms = ms;
+  }
+  if (q.error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
+  if (q.retired != (unsigned long long)n_items)
+    return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu items retired of %lld", q.retired, (long long)n_items);
+  return KRR_OK;
+}
+
 int krr_trace_images(int device, const krr_image* images, int32_t n_images, const double* Y0, const krr_launch* launch,
                      const krr_result* out, krr_stats* stats) {
   std::vector<krr::Image> ims;

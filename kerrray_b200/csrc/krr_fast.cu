@@ -44,4 +44,8 @@ const Variant* fast_variants(bool mixed, bool rk4, int* count) {
   return f64;
 }
 
+cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s) {
+  return mixed ? run_bisect<Mixed, 128, 1>(a, s) : run_bisect<Fast64, 128, 3>(a, s);
+}
+
 }  // namespace krr

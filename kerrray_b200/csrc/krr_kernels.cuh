@@ -184,6 +184,161 @@ __global__ void __launch_bounds__(MAXT, MINB)
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Edge bisection (scripts/study_edge_bisection.py:53-68): for each (case, polar angle phi) the
+// image radius rho is bisected between a bracket [lo, hi] (captured at lo, escaped at hi): a
+// photon at alpha = c_a + mid cos(phi), beta = c_b + mid sin(phi), mid = (lo + hi) / 2, is
+// traced; ESCAPED moves hi to mid, anything else moves lo to mid; a result that is neither
+// ESCAPED nor CAPTURED counts as a failure.  One lane owns one item and runs all its
+// iterations; lanes refill from the queue when their item is done.
+// ------------------------------------------------------------------------------------------
+struct EdgeCase {
+  Params P;
+  Frame F;
+  double c_alpha, c_beta;  // bracket centre in the image plane
+};
+
+struct EdgeArgs {
+  const EdgeCase* cases;
+  const int* item_case;
+  const double* cos_phi;
+  const double* sin_phi;
+  double* lo;
+  double* hi;
+  long long* failures;
+  long long n_items;
+  int iterations;
+  Queue* q;
+  int refill_threshold;
+  int grid, block;
+};
+
+template <class M>
+struct EdgeLane {
+  Ray<M> ry;
+  double lo, hi, mid, cphi, sphi;
+  long long fails;
+  int it, c;
+};
+
+template <class M>
+__device__ __forceinline__ void edge_start(const EdgeArgs& a, EdgeLane<M>& L) {
+  const EdgeCase& ec = a.cases[L.c];
+  L.mid = 0.5 * (L.lo + L.hi);
+  const double al = ec.c_alpha + L.mid * L.cphi;
+  const double be = ec.c_beta + L.mid * L.sphi;
+  double y0[8];
+  if (camera_state(ec.F, al, be, y0) != 0) atomicCAS(&a.q->error, 0, 6);
+  ray_init<M>(ec.P, y0, carter_initial(ec.P, y0), L.ry);
+}
+
+// The photon of the current iteration has terminated: update the bracket; start the next
+// iteration, or return false when the item is done.
+template <class M>
+__device__ __forceinline__ bool edge_next(const EdgeArgs& a, EdgeLane<M>& L) {
+  const int st = L.ry.state;
+  if (st != ESCAPED && st != CAPTURED) L.fails += 1;
+  if (st == ESCAPED) L.hi = L.mid; else L.lo = L.mid;
+  L.it += 1;
+  if (L.it >= a.iterations) return false;
+  edge_start<M>(a, L);
+  return true;
+}
+
+template <class M, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_bisect_edges(EdgeArgs a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  EdgeLane<M> L;
+  L.ry.state = FAILURE;
+  bool active = false, drained = false;
+  long long g = -1;
+  unsigned long long my_attempts = 0, my_accepted = 0, my_busy = 0, my_iters = 0;
+  auto finish_item = [&]() {
+    a.lo[g] = L.lo;
+    a.hi[g] = L.hi;
+    if (a.failures) a.failures[g] = L.fails;
+    atomicAdd(&a.q->retired, 1ull);
+    active = false;
+  };
+  while (true) {
+    const unsigned idle = __ballot_sync(FULL, !active);
+    const int n_idle = __popc(idle);
+    if (!drained && n_idle > 0 && (n_idle >= a.refill_threshold || n_idle == 32)) {
+      unsigned long long base = 0;
+      const int leader = __ffs(idle) - 1;
+      if ((int)lane == leader) base = atomicAdd(&a.q->head, (unsigned long long)n_idle);
+      base = __shfl_sync(FULL, base, leader);
+      if (base + (unsigned long long)n_idle >= (unsigned long long)a.n_items) drained = true;
+      if (!active) {
+        const unsigned long long mine = base + (unsigned long long)__popc(idle & lt_mask);
+        if (mine < (unsigned long long)a.n_items) {
+          g = (long long)mine;
+          L.c = a.item_case[g];
+          L.lo = a.lo[g];
+          L.hi = a.hi[g];
+          L.cphi = a.cos_phi[g];
+          L.sphi = a.sin_phi[g];
+          L.fails = 0;
+          L.it = 0;
+          active = a.iterations > 0;
+          if (active) {
+            edge_start<M>(a, L);
+            while (active && L.ry.state != RUNNING) active = edge_next<M>(a, L);
+          }
+          if (!active) finish_item();
+        }
+      }
+    }
+    const unsigned busy = __ballot_sync(FULL, active);
+    if (busy == 0) {
+      if (drained) break;
+      continue;
+    }
+    my_iters += 1;
+    if (active) {
+      my_busy += 1;
+      const int before = L.ry.n_steps;
+      attempt<M, false>(a.cases[L.c].P, L.ry, nullptr, nullptr);
+      my_attempts += 1;
+      my_accepted += (unsigned long long)(L.ry.n_steps - before);
+      if (L.ry.state != RUNNING) {
+        bool more = edge_next<M>(a, L);
+        while (more && L.ry.state != RUNNING) more = edge_next<M>(a, L);
+        if (!more) finish_item();
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    my_attempts += __shfl_down_sync(FULL, my_attempts, off);
+    my_accepted += __shfl_down_sync(FULL, my_accepted, off);
+    my_busy += __shfl_down_sync(FULL, my_busy, off);
+  }
+  if (lane == 0) {
+    atomicAdd(&a.q->attempts, my_attempts);
+    atomicAdd(&a.q->accepted, my_accepted);
+    atomicAdd(&a.q->busy_iters, my_busy);
+    atomicAdd(&a.q->lane_iters, my_iters * 32ull);
+  }
+}
+
+template <class M, int MAXT, int MINB>
+cudaError_t run_bisect(EdgeArgs a, cudaStream_t s) {
+  if (a.n_items <= 0) return cudaSuccess;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bisect_edges<M, MAXT, MINB>, MAXT, 0) != cudaSuccess || nb < 1)
+    return cudaErrorLaunchOutOfResources;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  a.block = MAXT;
+  a.grid = sms * nb;
+  k_bisect_edges<M, MAXT, MINB><<<a.grid, MAXT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 // Flag the pixels whose classification the FP64 re-trace must settle: every photon that did not
 // end ESCAPED or CAPTURED, and every pixel with a different code from one of its 8 neighbours
 // in the same image (the shadow edge).  Flagged global indices are appended to `list` (at most

@@ -17,6 +17,10 @@ const Variant* ref_variants(bool dtype32, bool rk4, int* count);
 cudaError_t fast_plain(bool mixed, bool rk4, const PlainArgs& a, int block, cudaStream_t s);
 const Variant* fast_variants(bool mixed, bool rk4, int* count);
 
+// Edge bisection launches (persistent, one item per lane).
+cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s);
+cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s);
+
 // Append the pixels to re-trace in FP64 (failures and the shadow edge) to `list`.
 cudaError_t flag_boundary(const Image* images, int n_images, long long total, const long long* state, long long* list,
                           Queue* q, cudaStream_t s);

@@ -20,6 +20,8 @@ const Variant* ref_variants(bool dtype32, bool rk4, int* count) {
   return rk4 ? v64rk4 : v64;
 }
 
+cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s) { return run_bisect<RefMode<double>, 128, 1>(a, s); }
+
 __global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, long long total,
                                 const long long* __restrict__ state, long long* __restrict__ list, Queue* q) {
   constexpr unsigned FULL = 0xffffffffu;

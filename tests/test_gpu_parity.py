@@ -297,3 +297,41 @@ def test_captured_graph_plan_equals_direct_launch() -> None:
             assert np.array_equal(sw.tensors["Y"].cpu().numpy(), direct.arrays["Y"])
             assert np.array_equal(sw.tensors["state"].cpu().numpy(), direct.arrays["state"])
         sw.close()
+
+
+@pytest.mark.parametrize("name", ["edge_bisection_a0.9_rtol1e-06", "edge_bisection_a0_rtol1e-08"])
+def test_edge_bisection_matches_reference(name: str) -> None:
+    """Device bisection (study_edge_bisection.py:53-68): same edge as the reference to ~rtol."""
+    d = golden(name)
+    st = K.Spacetime(1.0, float(d["spin"]))
+    rtol = float(d["rtol"])
+    r_mid, width, fails = K.bisect_edge(st, float(d["incl"]), float(d["r_o"]), rtol, d["centre_img"], d["angles"],
+                                        d["r_lo"], d["r_hi"], int(d["iterations"]))
+    assert fails == int(d["failures"]) == 0
+    assert np.allclose(width, d["width"], rtol=1e-3, atol=1e-14)
+    diff = np.abs(r_mid - d["r_num"])
+    err_gpu = r_mid * float(d["k"]) - d["r_ana"]
+    err_ref = d["r_num"] * float(d["k"]) - d["r_ana"]
+    print(name, "max |r_gpu - r_ref|", diff.max(), "rms edge error gpu", np.sqrt(np.mean(err_gpu**2)),
+          "ref", np.sqrt(np.mean(err_ref**2)))
+    assert diff.max() <= 2 * rtol
+    assert abs(np.sqrt(np.mean(err_gpu**2)) - np.sqrt(np.mean(err_ref**2))) <= 0.5 * rtol
+    for precision in ("fast64",):
+        r2, _, f2 = K.bisect_edge(st, float(d["incl"]), float(d["r_o"]), rtol, d["centre_img"], d["angles"],
+                                  d["r_lo"], d["r_hi"], int(d["iterations"]), precision=precision)
+        assert f2 == 0 and np.max(np.abs(r2 - d["r_num"])) <= 2 * rtol
+
+
+def test_batched_edge_bisection_over_cases() -> None:
+    """Several (spin, inclination, rtol) cases with 90 directions each in one launch."""
+    angles = 2 * np.pi * np.arange(90) / 90
+    cases = [K.edge_study(K.Spacetime(1.0, a), i, 1.0e5, rt, angles, bracket=(2.0, 8.0))
+             for a, i, rt in ((0.0, 17.0, 1e-6), (0.9, 60.0, 1e-6), (0.99, 85.0, 1e-6), (0.5, 60.0, 1e-8))]
+    res, stats = K.bisect_edges(cases, 36, precision="fast64")
+    assert stats["retired"] == 4 * 90
+    from kerrray_b200.bisect import edge_error
+
+    for case, (r_mid, width, fails) in zip(cases, res):
+        assert fails == 0 and np.all(width < 1e-9)
+        e = edge_error(case, r_mid)
+        assert e["rms_M"] < 20 * case.rtol, (case.spacetime.spin, e)
