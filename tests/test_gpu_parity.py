@@ -335,3 +335,27 @@ def test_batched_edge_bisection_over_cases() -> None:
         assert fails == 0 and np.all(width < 1e-9)
         e = edge_error(case, r_mid)
         assert e["rms_M"] < 20 * case.rtol, (case.spacetime.spin, e)
+
+
+def test_exact_checks_on_the_cuda_backend() -> None:
+    """The reference's Schwarzschild exact checks (configs/schwarzschild.yaml settings: rtol 1e-9,
+    atol 1e-11, 15 probes per iteration, brackets [2.5, 4] M and [4, 7] M, tolerance 1e-6 M):
+    photon sphere 3.000000014901 M (rel. 4.967e-9) and b_c 5.196152478456 M (rel. 1.073e-8) published."""
+    from kerrray_b200 import validation as V
+
+    integ = K.IntegratorOptions(method="rk45", rtol=1e-9, atol=1e-11)
+    term = K.TerminationOptions()
+    ps = V.photon_sphere(integ, term, r_lo=2.5, r_hi=4.0, tol=1e-6, max_iterations=60, n_probe=15)
+    assert ps.n_rays == 92 and ps.iterations == 6
+    assert abs(ps.radius - 3.0) / 3.0 < 1e-8, ps
+    assert abs(ps.radius - 3.000000014901) < 1e-9
+    (cb,) = V.critical_impacts(K.Spacetime(1.0, 0.0), integ, term, r0=1000.0, b_lo=4.0, b_hi=7.0, tol=1e-6,
+                               max_iterations=60, n_probe=15, directions=(True,))
+    assert abs(cb.b_c - V.CRITICAL_IMPACT_REFERENCE) / V.CRITICAL_IMPACT_REFERENCE < 2e-8, cb
+    assert abs(cb.b_c - 5.196152478456) < 1e-9
+    # Kerr: prograde and retrograde thresholds bracket the analytic critical impact parameters.
+    st = K.Spacetime(1.0, 0.9)
+    pro, retro = V.critical_impacts(st, integ, term, r0=1000.0, b_lo=1.0, b_hi=9.0, tol=1e-6, max_iterations=60,
+                                    n_probe=15)
+    b_pro, b_retro = K.critical_impact_parameters(st)
+    assert abs(pro.b_c - b_pro) < 1e-5 and abs(retro.b_c - b_retro) < 1e-5
