@@ -306,7 +306,13 @@ def run_ours(args) -> None:
 
     specs = workload_specs(K, args.workload)
     total = sum(s.n_rays for s in specs)
-    tuned, tune_report = K.autotune(specs, precision=args.precision, device=local)
+    if args.launch:
+        variant, refill = (int(x) for x in args.launch.split(":"))
+        tuned = K.LaunchConfig(variant=variant, refill_threshold=refill)
+        info = [v for v in K.list_variants(args.precision, specs[0].integ, specs[0].term, local) if v["variant"] == variant]
+        tune_report = {"trials": [{**info[0], "refill_threshold": refill, "ms": None}]}
+    else:
+        tuned, tune_report = K.autotune(specs, precision=args.precision, device=local)
     sweep = K.DeviceSweep(specs, precision=args.precision, device=local, launch=tuned)
     stream = torch.cuda.current_stream(local)
     for _ in range(args.warmup):
@@ -421,6 +427,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sweep")
     ap.add_argument("--precision", choices=("reference", "fast64", "mixed"), default="fast64")
+    ap.add_argument("--launch", default="", help="VARIANT:REFILL launch shape instead of the autotuner's choice")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the device launches only (no plain-kernel, end-to-end or CPU legs)")
     args = ap.parse_args()
