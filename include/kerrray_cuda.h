@@ -230,6 +230,36 @@ KRR_API int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_c
                              int64_t* failures, int64_t n_items, int32_t iterations, int32_t precision,
                              krr_stats* stats);
 
+/* The lensing map of one observer, differentiated: for n image points (alpha, beta) the terminal
+ * celestial direction (theta_e, phi_e) -- theta and phi located on the termination surface
+ * (escape radius, or capture radius) from the last accepted state by one step along the flow --
+ * and its Jacobian d(theta_e, phi_e)/d(alpha, beta, spin, theta_o [rad]) (jac: n x 2 x 4), by the
+ * adjoint of the discretised Dormand-Prince 5(4) map over the recorded accepted steps with the
+ * controller held fixed, checkpoints every `checkpoint_every` steps and recomputation in the
+ * reverse sweep.  FP64.  No counterpart in the reference (its gradients are finite
+ * differences of raytracing/backends/numba_backend.py runs).  Device buffers; `workspace` holds
+ * the tape (krr_lensing_workspace_size bytes) and must be kept for krr_lensing_replay.
+ * status[k]: 0 ok, 1 more accepted steps than tape_capacity, 2 neither ESCAPED nor CAPTURED. */
+typedef struct krr_lens_params {
+  double mass, spin;
+  double radius, inclination_deg, phi_deg;
+  krr_options options;  /* rk45, float64, no events */
+  int32_t checkpoint_every;  /* K, 1..64 */
+  int32_t tape_capacity;     /* accepted steps recorded per ray */
+} krr_lens_params;
+KRR_API size_t krr_lensing_workspace_size(int64_t n, int32_t tape_capacity, int32_t checkpoint_every);
+KRR_API int krr_lensing_adjoint(int device, const krr_lens_params* params, const double* d_alpha, const double* d_beta,
+                                int64_t n, double* d_theta, double* d_phi, double* d_jac, int64_t* d_state,
+                                int64_t* d_n_steps, int32_t* d_status, void* workspace, size_t workspace_bytes,
+                                void* stream);
+/* Re-run the map with the step sequence recorded by the last krr_lensing_adjoint call on this
+ * workspace (same n, states and step counts), for other (alpha, beta, spin, inclination): the
+ * discrete map the adjoint differentiates, without the controller. */
+KRR_API int krr_lensing_replay(int device, const krr_lens_params* params, const double* d_alpha, const double* d_beta,
+                               int64_t n, const int64_t* d_state, const int64_t* d_n_steps, double* d_theta,
+                               double* d_phi, int32_t* d_status, const void* workspace, size_t workspace_bytes,
+                               void* stream);
+
 /* Allocation-free form of krr_trace_images_device.  No counterpart in the reference.  For
  * callers that cannot allocate device memory on this path (an application that owns a fixed
  * device-memory budget, work enqueued on a stream another library captures, a plug-in whose

@@ -27,6 +27,7 @@ EXPORTS = (
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
     "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
     "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy", "krr_bisect_edges",
+    "krr_lensing_workspace_size", "krr_lensing_adjoint", "krr_lensing_replay",
 )
 
 

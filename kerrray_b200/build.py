@@ -32,6 +32,7 @@ UNITS = {
     "krr_abi.cu": [],
     "krr_peak.cu": [],
     "krr_noalloc.cu": [],
+    "krr_adjoint.cu": ["-fmad=false"],
 }
 
 

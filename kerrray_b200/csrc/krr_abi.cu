@@ -792,6 +792,87 @@ int krr_plan_destroy(krr_plan* plan) {
   return KRR_OK;
 }
 
+size_t krr_lensing_workspace_size(int64_t n, int32_t tape_capacity, int32_t checkpoint_every) {
+  if (n < 0 || tape_capacity < 1 || checkpoint_every < 1) return 0;
+  const size_t ck = (size_t)(tape_capacity / checkpoint_every + 1) * 6;
+  return round256((size_t)n * tape_capacity * 8) + round256((size_t)n * ck * 8);
+}
+
+static int lens_launch(const krr_lens_params* p, int64_t n, krr::LensLaunch& L, size_t workspace_bytes) {
+  if (!p) return fail(KRR_ERR_INVALID, "params must not be NULL");
+  int rc = validate_spacetime(p->mass, p->spin);
+  if (!rc) rc = validate_options(&p->options);
+  if (rc) return rc;
+  if (p->options.method != 0 || p->options.dtype != 0 || p->options.disk_plane)
+    return fail(KRR_ERR_UNSUPPORTED, "the lensing adjoint integrates with rk45 in float64 without events");
+  if (p->checkpoint_every < 1 || p->checkpoint_every > 64)
+    return fail(KRR_ERR_INVALID, "checkpoint_every must lie in [1, 64], got %d", p->checkpoint_every);
+  if (p->tape_capacity < 1) return fail(KRR_ERR_INVALID, "tape_capacity must be >= 1");
+  if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0");
+  if (workspace_bytes < krr_lensing_workspace_size(n, p->tape_capacity, p->checkpoint_every))
+    return fail(KRR_ERR_INVALID, "workspace too small for the tape");
+  krr_camera cam{p->radius, p->inclination_deg, p->phi_deg, 1.0, 2};
+  krr::Frame F{};
+  rc = make_frame(p->mass, p->spin, &cam, F);
+  if (rc) return rc;
+  L.P = make_params(p->mass, p->spin, &p->options);
+  L.spin = p->spin;
+  L.mass = p->mass;
+  L.r_o = F.r_o;
+  L.th_o = F.th_o;
+  L.ph_o = F.ph_o;
+  L.K = p->checkpoint_every;
+  L.cap = p->tape_capacity;
+  L.n = n;
+  return KRR_OK;
+}
+
+int krr_lensing_adjoint(int device, const krr_lens_params* params, const double* d_alpha, const double* d_beta,
+                        int64_t n, double* d_theta, double* d_phi, double* d_jac, int64_t* d_state, int64_t* d_n_steps,
+                        int32_t* d_status, void* workspace, size_t workspace_bytes, void* stream) {
+  krr::LensLaunch L{};
+  int rc = lens_launch(params, n, L, workspace_bytes);
+  if (rc) return rc;
+  if (n == 0) return KRR_OK;
+  if (!d_alpha || !d_beta || !d_theta || !d_phi || !d_jac || !d_state || !d_n_steps || !d_status || !workspace)
+    return fail(KRR_ERR_INVALID, "device buffers must not be NULL");
+  KRR_CUDA(cudaSetDevice(device));
+  L.alpha = d_alpha;
+  L.beta = d_beta;
+  L.theta = d_theta;
+  L.phi = d_phi;
+  L.jac = d_jac;
+  L.state = reinterpret_cast<long long*>(d_state);
+  L.n_steps = reinterpret_cast<long long*>(d_n_steps);
+  L.status = d_status;
+  L.tape_h = static_cast<double*>(workspace);
+  L.tape_ck = reinterpret_cast<double*>(static_cast<char*>(workspace) + round256((size_t)n * L.cap * 8));
+  KRR_CUDA(krr::lensing_adjoint(L, false, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
+int krr_lensing_replay(int device, const krr_lens_params* params, const double* d_alpha, const double* d_beta,
+                       int64_t n, const int64_t* d_state, const int64_t* d_n_steps, double* d_theta, double* d_phi,
+                       int32_t* d_status, const void* workspace, size_t workspace_bytes, void* stream) {
+  krr::LensLaunch L{};
+  int rc = lens_launch(params, n, L, workspace_bytes);
+  if (rc) return rc;
+  if (n == 0) return KRR_OK;
+  if (!d_alpha || !d_beta || !d_theta || !d_phi || !d_state || !d_n_steps || !d_status || !workspace)
+    return fail(KRR_ERR_INVALID, "device buffers must not be NULL");
+  KRR_CUDA(cudaSetDevice(device));
+  L.alpha = d_alpha;
+  L.beta = d_beta;
+  L.theta = d_theta;
+  L.phi = d_phi;
+  L.state = const_cast<long long*>(reinterpret_cast<const long long*>(d_state));
+  L.n_steps = const_cast<long long*>(reinterpret_cast<const long long*>(d_n_steps));
+  L.status = d_status;
+  L.tape_h = const_cast<double*>(static_cast<const double*>(workspace));
+  KRR_CUDA(krr::lensing_adjoint(L, true, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
 int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, const int32_t* item_case,
                      const double* cos_phi, const double* sin_phi, double* lo, double* hi, int64_t* failures,
                      int64_t n_items, int32_t iterations, int32_t precision, krr_stats* stats) {

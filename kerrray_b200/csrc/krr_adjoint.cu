@@ -1,0 +1,357 @@
+// Adjoint of the discretised Dormand-Prince 5(4) map: derivatives of a ray's terminal celestial
+// direction with respect to (alpha, beta, spin, inclination).
+//
+// For each ray (one thread):
+//   1. the camera state y0 and its Jacobian d y0 / d(alpha, beta, a, theta_o) by forward-mode
+//      dual numbers through the camera (raytracing/camera.py:225-381);
+//   2. the forward integration in FP64 (the Fast64 arithmetic and the reference's controller),
+//      recording every accepted step size and the state every K accepted steps (checkpoints);
+//   3. the output: theta and phi at the termination surface r_s (the escape radius, or the
+//      capture radius r_plus + epsilon), located from the final accepted state y_N by one
+//      linear step along the flow: x_e = x_N - (f_x / f_r)(r_N - r_s) (the event-time
+//      correction: d lambda_e = -d r / f_r);
+//   4. the reverse sweep over the recorded step sequence with the controller held fixed: each
+//      K-step segment is recomputed from its checkpoint, then the adjoint of each DP5 step runs
+//      back through its six stages; the right-hand side's vector-Jacobian product uses the
+//      closed-form momentum derivatives and forward-mode duals for the (r, theta, a)
+//      derivatives of the 15 metric terms;
+//   5. the chain through the camera Jacobian.
+// Both outputs (theta_e, phi_e) are swept together (two cotangent rows).
+#include <cuda_runtime.h>
+
+#include "krr_device.cuh"
+#include "krr_dual.cuh"
+#include "krr_launch.h"
+#include <math_constants.h>
+
+namespace krr {
+
+namespace {
+
+constexpr int NC = 2;     // cotangent rows: theta_e, phi_e
+constexpr int NX = NV + 2;  // adjoint state: the six integrated components, p_t, p_phi
+constexpr int XPT = NV, XPPH = NV + 1;
+
+// d(v . f)/d(state, a) at (r, theta, p_t, p_r, p_theta, p_phi) for NC cotangents v (each over
+// the six integrated components of f); accumulates into xbar and abar.
+__device__ void rhs_vjp(double m, double a, double r, double th, double pt, double pr, double pth, double pph,
+                        const double v[NC][NV], double xbar[NC][NX], double abar[NC]) {
+  Dual<3> g[15];
+  metric_terms<Dual<3>>(Dual<3>::var(r, 0), Dual<3>::var(th, 1), Dual<3>::var(a, 2), m, g);
+  if (pph == 0.0) {  // the polar-axis guard of the right-hand side
+    g[4] = Dual<3>(0.0);
+    g[9] = Dual<3>(0.0);
+    g[14] = Dual<3>(0.0);
+  }
+  const double pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const double vt = v[c][CT], vr = v[c][CR], vth = v[c][CTH], vph = v[c][CPH], vpr = v[c][CPR], vpth = v[c][CPTH];
+    double gb[15];
+    gb[0] = vt * pt;
+    gb[1] = vt * pph + vph * pt;
+    gb[2] = vr * pr;
+    gb[3] = vth * pth;
+    gb[4] = vph * pph;
+    gb[5] = -0.5 * vpr * pt2;
+    gb[6] = -vpr * ptpph;
+    gb[7] = -0.5 * vpr * pr2;
+    gb[8] = -0.5 * vpr * pth2;
+    gb[9] = -0.5 * vpr * pph2;
+    gb[10] = -0.5 * vpth * pt2;
+    gb[11] = -vpth * ptpph;
+    gb[12] = -0.5 * vpth * pr2;
+    gb[13] = -0.5 * vpth * pth2;
+    gb[14] = -0.5 * vpth * pph2;
+    double dr = 0.0, dth = 0.0, da = 0.0;
+#pragma unroll
+    for (int j = 0; j < 15; ++j) {
+      dr = fma(gb[j], g[j].d[0], dr);
+      dth = fma(gb[j], g[j].d[1], dth);
+      da = fma(gb[j], g[j].d[2], da);
+    }
+    xbar[c][CR] += dr;
+    xbar[c][CTH] += dth;
+    abar[c] += da;
+    const double g0 = g[0].v, g1 = g[1].v, g2 = g[2].v, g3 = g[3].v, g4 = g[4].v;
+    xbar[c][XPT] += vt * g0 + vph * g1 - vpr * (g[5].v * pt + g[6].v * pph) - vpth * (g[10].v * pt + g[11].v * pph);
+    xbar[c][XPPH] += vt * g1 + vph * g4 - vpr * (g[6].v * pt + g[9].v * pph) - vpth * (g[11].v * pt + g[14].v * pph);
+    xbar[c][CPR] += vr * g2 - (vpr * g[7].v + vpth * g[12].v) * pr;
+    xbar[c][CPTH] += vth * g3 - (vpr * g[8].v + vpth * g[13].v) * pth;
+  }
+}
+
+// Stage coefficients of the Dormand-Prince 5(4) map in the 1..6 numbering of its new stages:
+// stage input s (s = 1..5) uses a[s][j] for j < s; the new state uses b[j].
+__device__ __forceinline__ double dp_a(int s, int j) {
+  const double A[6][6] = {
+      {dp::A10, 0, 0, 0, 0, 0},
+      {dp::A20, dp::A21, 0, 0, 0, 0},
+      {dp::A30, dp::A31, dp::A32, 0, 0, 0},
+      {dp::A40, dp::A41, dp::A42, dp::A43, 0, 0},
+      {dp::A50, dp::A51, dp::A52, dp::A53, dp::A54, 0},
+      {dp::B0, 0.0, dp::B2, dp::B3, dp::B4, dp::B5},
+  };
+  return A[s][j];
+}
+
+struct LensArgs {
+  Params P;  // integrator/termination parameters (spin and mass included)
+  double spin, mass, r_o, th_o, ph_o;
+  int K;    // checkpoint interval (accepted steps)
+  int cap;  // tape capacity (accepted steps per ray)
+  const double* alpha;
+  const double* beta;
+  long long n;
+  double* theta;
+  double* phi;
+  double* jac;  // (n, 2, 4): rows theta_e, phi_e; columns alpha, beta, spin, theta_o (rad)
+  long long* state;
+  long long* n_steps;
+  int* status;  // 0 ok, 1 tape full, 2 ended neither ESCAPED nor CAPTURED
+  double* tape_h;   // (n, cap)
+  double* tape_ck;  // (n, cap / K + 1, NV)
+};
+
+__device__ __forceinline__ double surface_radius(const Params& P, int state) {
+  return state == ESCAPED ? P.r_escape : P.r_capture;
+}
+
+// One fixed step of size h from (y, f = f(y)): the forward map the adjoint differentiates; with
+// recorded stage sums for the reverse pass.
+__device__ __forceinline__ void fixed_step(const Params& P, Ray<Fast64>& ry, double h, double acc[6][NV],
+                                           double k[6][NV]) {
+  double yn[NV];
+  Trig tr;
+  dp_stages<Fast64, false>(P, ry, h, k[0], k[1], k[2], k[3], k[4], k[5], yn, tr, acc);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    ry.y[i] = yn[i];
+    ry.f[i] = k[5][i];
+  }
+}
+
+__global__ void __launch_bounds__(128) k_lensing_adjoint(LensArgs A) {
+  const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (ray >= A.n) return;
+  const Params& P = A.P;
+  const double m = A.mass, a = A.P.a;
+  // 1. camera and its Jacobian in (alpha, beta, a, theta_o)
+  Dual<4> y0d[8];
+  camera_state_t<Dual<4>>(Dual<4>::var(A.alpha[ray], 0), Dual<4>::var(A.beta[ray], 1), Dual<4>::var(a, 2),
+                          Dual<4>::var(A.th_o, 3), A.r_o, A.ph_o, m, y0d);
+  double y0[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) y0[i] = y0d[i].v;
+  // 2. forward pass with the controller; record step sizes and checkpoints
+  double* tape_h = A.tape_h + ray * (long long)A.cap;
+  const int n_ck = A.cap / A.K + 1;
+  double* tape_ck = A.tape_ck + ray * (long long)n_ck * NV;
+  Ray<Fast64> ry;
+  ray_init<Fast64>(P, y0, carter_initial(P, y0), ry);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) tape_ck[i] = ry.y[i];
+  int status = 0;
+  while (ry.state == RUNNING) {
+    const int before = ry.n_steps;
+    attempt<Fast64, false>(P, ry, nullptr, nullptr);
+    if (ry.n_steps != before) {
+      const int n = ry.n_steps;
+      if (n > A.cap) {
+        status = 1;
+        break;
+      }
+      tape_h[n - 1] = ry.h_taken;
+      if (n % A.K == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) tape_ck[(n / A.K) * NV + i] = ry.y[i];
+      }
+    }
+  }
+  const int N = ry.n_steps;
+  A.state[ray] = ry.state;
+  A.n_steps[ray] = N;
+  if (status == 0 && ry.state != ESCAPED && ry.state != CAPTURED) status = 2;
+  // 3. the output at the termination surface and its cotangents
+  const double rs = surface_radius(P, ry.state);
+  const double dr = ry.y[CR] - rs;
+  const double fr = ry.f[CR];
+  A.theta[ray] = ry.y[CTH] - ry.f[CTH] / fr * dr;
+  A.phi[ray] = ry.y[CPH] - ry.f[CPH] / fr * dr;
+  double* J = A.jac + ray * 8;
+  if (status != 0) {
+    A.status[ray] = status;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) J[i] = CUDART_NAN;
+    return;
+  }
+  const int out_comp[NC] = {CTH, CPH};
+  double xbar[NC][NX];
+  double abar[NC] = {0.0, 0.0};
+  {
+    double v[NC][NV];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+#pragma unroll
+      for (int i = 0; i < NX; ++i) xbar[c][i] = 0.0;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) v[c][i] = 0.0;
+      const double fx = ry.f[out_comp[c]];
+      xbar[c][out_comp[c]] = 1.0;
+      xbar[c][CR] -= fx / fr;
+      v[c][out_comp[c]] = -dr / fr;
+      v[c][CR] = dr * fx / (fr * fr);
+    }
+    rhs_vjp(m, a, ry.y[CR], ry.y[CTH], ry.pt, ry.y[CPR], ry.y[CPTH], ry.pph, v, xbar, abar);
+    if (ry.state == CAPTURED) {  // r_s = r_plus(a) + epsilon moves with a
+      const double drp_da = -a / sqrt(m * m - a * a);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) abar[c] += ry.f[out_comp[c]] / fr * drp_da;
+    }
+  }
+  // 4. reverse sweep, segment by segment from the last
+  double seg[64][NV];  // states of one segment (K <= 64)
+  for (int c0 = (N - 1) / A.K; c0 >= 0; --c0) {
+    const int n0 = c0 * A.K, n1 = min(N, n0 + A.K);
+    Ray<Fast64> rs_ray = ry;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) rs_ray.y[i] = tape_ck[c0 * NV + i];
+    Fast64::init_rhs(P, rs_ray.y, rs_ray.pt, rs_ray.pph, rs_ray.sh, rs_ray.f, rs_ray.tr);
+    double acc[6][NV], k[6][NV];
+    for (int n = n0; n < n1; ++n) {
+#pragma unroll
+      for (int i = 0; i < NV; ++i) seg[n - n0][i] = rs_ray.y[i];
+      if (n + 1 < n1) fixed_step(P, rs_ray, tape_h[n], acc, k);
+    }
+    for (int n = n1 - 1; n >= n0; --n) {
+      const double h = tape_h[n];
+      Ray<Fast64> st = ry;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) st.y[i] = seg[n - n0][i];
+      Fast64::init_rhs(P, st.y, st.pt, st.pph, st.sh, st.f, st.tr);
+      fixed_step(P, st, h, acc, k);
+      // Reverse of: Y_s = y + h acc_s (s = 1..5 -> k_s = f(Y_s)); y_new = y + h acc_6; the
+      // stage-s sums are linear in k_0 = f(y) and k_1..k_{s-1} with the tableau weights.
+      double kbar[NC][6][NV];  // cotangents of k_0..k_5 (k_0 = f(y), k_s = f(Y_s))
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int j = 0; j < 6; ++j)
+#pragma unroll
+          for (int i = 0; i < NV; ++i) kbar[c][j][i] = h * dp_a(5, j) * xbar[c][i];
+      for (int s = 5; s >= 1; --s) {  // stage inputs Y_s, s = 5..1, produced k_s
+        double v[NC][NV], ybar_s[NC][NX];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+#pragma unroll
+          for (int i = 0; i < NV; ++i) v[c][i] = kbar[c][s][i];
+#pragma unroll
+          for (int i = 0; i < NX; ++i) ybar_s[c][i] = 0.0;
+        }
+        const int sm = s - 1;  // acc index of stage input s
+        // The stage input exactly as the forward formed it (upd<Fast64>: one fused step).
+        const double Yr = fma(h, acc[sm][CR], seg[n - n0][CR]);
+        const double Yth = fma(h, acc[sm][CTH], seg[n - n0][CTH]);
+        const double Ypr = fma(h, acc[sm][CPR], seg[n - n0][CPR]);
+        const double Ypth = fma(h, acc[sm][CPTH], seg[n - n0][CPTH]);
+        rhs_vjp(m, a, Yr, Yth, ry.pt, Ypr, Ypth, ry.pph, v, ybar_s, abar);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+#pragma unroll
+          for (int i = 0; i < NX; ++i) xbar[c][i] += ybar_s[c][i];
+          for (int j = 0; j < s; ++j) {
+            const double w = h * dp_a(sm, j);
+            if (w != 0.0) {
+#pragma unroll
+              for (int i = 0; i < NV; ++i) kbar[c][j][i] += w * ybar_s[c][i];
+            }
+          }
+        }
+      }
+      {  // k_0 = f(y)
+        double v[NC][NV];
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int i = 0; i < NV; ++i) v[c][i] = kbar[c][0][i];
+        rhs_vjp(m, a, seg[n - n0][CR], seg[n - n0][CTH], ry.pt, seg[n - n0][CPR], seg[n - n0][CPTH], ry.pph, v, xbar,
+                abar);
+      }
+    }
+  }
+  // 5. chain through the camera: d/d(alpha, beta, a, theta_o), then a = spin * M
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    double g[4] = {0.0, 0.0, 0.0, 0.0};
+    const int map[8] = {CT, CR, CTH, CPH, XPT, CPR, CPTH, XPPH};  // 8-state slot -> adjoint slot
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double xb = xbar[c][map[i]];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) g[p] = fma(xb, y0d[i].d[p], g[p]);
+    }
+    g[2] += abar[c];
+    J[c * 4 + 0] = g[0];
+    J[c * 4 + 1] = g[1];
+    J[c * 4 + 2] = g[2] * m;
+    J[c * 4 + 3] = g[3];
+  }
+  A.status[ray] = 0;
+}
+
+// Replay: the same camera and the recorded step sequence without the controller (the map the
+// adjoint differentiates), for finite-difference checks.
+__global__ void __launch_bounds__(128) k_lensing_replay(LensArgs A) {
+  const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (ray >= A.n) return;
+  const Params& P = A.P;
+  double y0[8];
+  camera_state_t<double>(A.alpha[ray], A.beta[ray], A.P.a, A.th_o, A.r_o, A.ph_o, A.mass, y0);
+  Ray<Fast64> ry;
+  ray_init<Fast64>(P, y0, carter_initial(P, y0), ry);
+  const long long N = A.n_steps[ray];
+  const double* tape_h = A.tape_h + ray * (long long)A.cap;
+  double acc[6][NV], k[6][NV];
+  for (long long n = 0; n < N; ++n) fixed_step(P, ry, tape_h[n], acc, k);
+  const int state = (int)A.state[ray];
+  const double rs = surface_radius(P, state);
+  const double dr = ry.y[CR] - rs;
+  A.theta[ray] = ry.y[CTH] - ry.f[CTH] / ry.f[CR] * dr;
+  A.phi[ray] = ry.y[CPH] - ry.f[CPH] / ry.f[CR] * dr;
+  A.status[ray] = 0;
+}
+
+}  // namespace
+
+cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s) {
+  if (L.n <= 0) return cudaSuccess;
+  LensArgs A{};
+  A.P = L.P;
+  A.spin = L.spin;
+  A.mass = L.mass;
+  A.r_o = L.r_o;
+  A.th_o = L.th_o;
+  A.ph_o = L.ph_o;
+  A.K = L.K;
+  A.cap = L.cap;
+  A.alpha = L.alpha;
+  A.beta = L.beta;
+  A.n = L.n;
+  A.theta = L.theta;
+  A.phi = L.phi;
+  A.jac = L.jac;
+  A.state = L.state;
+  A.n_steps = L.n_steps;
+  A.status = L.status;
+  A.tape_h = L.tape_h;
+  A.tape_ck = L.tape_ck;
+  const int block = 128;
+  const unsigned grid = (unsigned)((L.n + block - 1) / block);
+  if (replay)
+    k_lensing_replay<<<grid, block, 0, s>>>(A);
+  else
+    k_lensing_adjoint<<<grid, block, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace krr

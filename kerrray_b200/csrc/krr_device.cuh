@@ -421,6 +421,7 @@ struct Ray {
   S pt, pph; // constants of the motion
   K f[NV];   // FSAL right-hand side at y
   S h;       // proposed step (working type, like the reference's h)
+  S h_taken; // step of the last accepted attempt
   double lam;
   double m_null, m_q;
   Refs ref;
@@ -538,6 +539,81 @@ __device__ __forceinline__ typename M::N step_factor(typename M::N en, bool reje
   return factor;
 }
 
+// The stages of one step of size h from ry.y with FSAL stage ry.f (numba_kernel.py:201-257):
+// k1..k5 (DP5; k1..k3 for RK4), the candidate state yn and k6 = f(yn).  With acc_rec, the
+// stage-input sums acc_s (stage input = y + h * acc_s) are recorded for s = 1..6 (the adjoint
+// rebuilds the stage inputs from them).
+template <class M, bool RK4>
+__device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k1[NV],
+                                          typename M::K k2[NV], typename M::K k3[NV], typename M::K k4[NV],
+                                          typename M::K k5[NV], typename M::K k6[NV], typename M::S yn[NV], Trig& tr,
+                                          typename M::K (*acc_rec)[NV] = nullptr) {
+  using K = typename M::K;
+  const K* k0 = ry.f;
+  auto c = [](double x) { return (K)x; };
+  K acc[NV];
+  auto store = [&](int s) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc_rec[s][i] = acc[i];
+  };
+  // Stage inputs: the reference's sums (same terms and order, zero coefficients skipped);
+  // madd fuses them in the fast modes and rounds each operation in the reference modes.
+  if constexpr (!RK4) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = c(dp::A10) * k0[i];
+    if (acc_rec) store(0);
+    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = madd<M>(c(dp::A20) * k0[i], c(dp::A21), k1[i]);
+    if (acc_rec) store(1);
+    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = madd<M>(madd<M>(c(dp::A30) * k0[i], c(dp::A31), k1[i]), c(dp::A32), k2[i]);
+    if (acc_rec) store(2);
+    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      const K a = madd<M>(c(dp::A40) * k0[i], c(dp::A41), k1[i]);
+      acc[i] = madd<M>(madd<M>(a, c(dp::A42), k2[i]), c(dp::A43), k3[i]);
+    }
+    if (acc_rec) store(3);
+    M::template stage<false>(P, ry, h, acc, k4, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      const K a = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
+      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::A52), k2[i]), c(dp::A53), k3[i]), c(dp::A54), k4[i]);
+    }
+    if (acc_rec) store(4);
+    M::template stage<false>(P, ry, h, acc, k5, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      const K a = madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]);
+      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::B3), k3[i]), c(dp::B4), k4[i]), c(dp::B5), k5[i]);
+    }
+    if (acc_rec) store(5);
+    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k0[i];
+    if (acc_rec) store(0);
+    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k1[i];
+    if (acc_rec) store(1);
+    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = c(1.0) * k2[i];
+    if (acc_rec) store(2);
+    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      acc[i] = madd<M>(madd<M>(madd<M>(c(dp::RK4_B0) * k0[i], c(dp::RK4_B1), k1[i]), c(dp::RK4_B2), k2[i]),
+                       c(dp::RK4_B3), k3[i]);
+    if (acc_rec) store(5);
+    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
+  }
+}
+
 // One step attempt (numba_kernel.py:376-455): DP5(4) (or RK4) step, error norm, controller,
 // accept/reject, diagnostics and classification.  Returns with ry.state updated.
 template <class M, bool RK4>
@@ -559,54 +635,8 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   S yn[NV];
   Trig tr;
   const K* k0 = ry.f;
-  // Stage inputs: the reference's sums (same terms and order, zero coefficients skipped);
-  // madd fuses them in the fast modes and rounds each operation in the reference modes.
   auto c = [](double x) { return (K)x; };
-  K acc[NV];
-  if constexpr (!RK4) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = c(dp::A10) * k0[i];
-    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = madd<M>(c(dp::A20) * k0[i], c(dp::A21), k1[i]);
-    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = madd<M>(madd<M>(c(dp::A30) * k0[i], c(dp::A31), k1[i]), c(dp::A32), k2[i]);
-    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const K a = madd<M>(c(dp::A40) * k0[i], c(dp::A41), k1[i]);
-      acc[i] = madd<M>(madd<M>(a, c(dp::A42), k2[i]), c(dp::A43), k3[i]);
-    }
-    M::template stage<false>(P, ry, h, acc, k4, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const K a = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
-      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::A52), k2[i]), c(dp::A53), k3[i]), c(dp::A54), k4[i]);
-    }
-    M::template stage<false>(P, ry, h, acc, k5, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      const K a = madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]);
-      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::B3), k3[i]), c(dp::B4), k4[i]), c(dp::B5), k5[i]);
-    }
-    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
-  } else {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k0[i];
-    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k1[i];
-    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = c(1.0) * k2[i];
-    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
-#pragma unroll
-    for (int i = 0; i < NV; ++i)
-      acc[i] = madd<M>(madd<M>(madd<M>(c(dp::RK4_B0) * k0[i], c(dp::RK4_B1), k1[i]), c(dp::RK4_B2), k2[i]),
-                       c(dp::RK4_B3), k3[i]);
-    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
-  }
+  dp_stages<M, RK4>(P, ry, h, k1, k2, k3, k4, k5, k6, yn, tr);
   bool finite = true;
 #pragma unroll
   for (int i = 0; i < NV; ++i) finite = finite && finite_(yn[i]) && finite_(k6[i]);
@@ -671,6 +701,7 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   const double lam_old = ry.lam;
   ry.lam = last ? P.lambda_max : ry.lam + (double)h_eff;
   ry.n_steps += 1;
+  ry.h_taken = h_eff;
   // E and L_z drifts are identically zero (p_t, p_phi never change); Q and the null error:
   ry.m_q = py_max(ry.m_q, fabs(carter<M>(P, ry) - ry.ref.q0) / py_max(fabs(ry.ref.q0), ry.ref.fq));
   ry.m_null = py_max(ry.m_null, null_error<M>(ry) / ry.ref.fe2);

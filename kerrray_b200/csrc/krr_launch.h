@@ -21,6 +21,26 @@ const Variant* fast_variants(bool mixed, bool rk4, int* count);
 cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s);
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s);
 
+// Lensing-map adjoint (krr_adjoint.cu): derivatives of the terminal celestial direction with
+// respect to (alpha, beta, spin, theta_o); replay = the recorded step sequence without them.
+struct LensLaunch {
+  Params P;
+  double spin, mass, r_o, th_o, ph_o;
+  int K, cap;
+  const double* alpha;
+  const double* beta;
+  long long n;
+  double* theta;
+  double* phi;
+  double* jac;
+  long long* state;
+  long long* n_steps;
+  int* status;
+  double* tape_h;
+  double* tape_ck;
+};
+cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s);
+
 // Append the pixels to re-trace in FP64 (failures and the shadow edge) to `list`.
 cudaError_t flag_boundary(const Image* images, int n_images, long long total, const long long* state, long long* list,
                           Queue* q, cudaStream_t s);
