@@ -53,6 +53,11 @@ WORKLOADS = {
     "sweep": WORKLOAD,
     "sweep128": "the 36 128^2 images of the sweep (a*{0,0.5,0.9,0.99} x i{17,60,85} x rtol{1e-6,1e-8,1e-10})",
     "spin99_1024": "a*=0.99, i=85deg, r_o=1000 M, +-8 M, 1024^2, rtol 1e-6, atol 1e-8",
+    "spin99_2048": "a*=0.99, i=85deg, r_o=1000 M, +-8 M, 2048^2, rtol 1e-6, atol 1e-8",
+    "bisect": ("batched edge bisection: a*{0,0.5,0.9,0.99} x i{17,60,85}deg x 1440 polar angles x rtol{1e-6,1e-8,"
+               "1e-10}, rho in [2, 8] M about the Bardeen centroid / k, 36 halvings, r_o = 1e5 M"),
+    "lensing": ("lensing-map adjoint: a*=0.8, i=60deg, r_o=1000 M, 256^2 over +-12 M, escaped rays > 3 px from the "
+                "shadow edge, rtol 1e-10, checkpoints every 32 accepted steps"),
 }
 
 
@@ -61,8 +66,8 @@ def workload_specs(K, name: str):
         return sweep_specs(K)
     if name == "sweep128":
         return sweep_specs(K, resolutions=(128,))
-    if name == "spin99_1024":
-        cam = K.Camera(radius=1000.0, inclination_deg=85.0, fov=8.0, resolution=1024)
+    if name in ("spin99_1024", "spin99_2048"):
+        cam = K.Camera(radius=1000.0, inclination_deg=85.0, fov=8.0, resolution=int(name[-4:]))
         integ = K.IntegratorOptions(method="rk45", rtol=1e-6, atol=1e-8)
         return [K.ImageSpec(K.Spacetime(1.0, 0.99), cam, integ, K.TerminationOptions())]
     raise ValueError(name)
@@ -252,12 +257,41 @@ def _timed_steps(sweep, steps: int, stream, flush) -> list[float]:
     return out
 
 
-def mixed_vs_plain(K, local: int, stream, flush) -> dict:
-    """Mixed persistent + FP64 re-trace against the plain FP64 kernel on the 1024^2, a*=0.99,
-    i=85 deg image (rtol 1e-6): rays/s of each and whether the two shadow masks are identical."""
+def edge_rms_px(K, spec, state: np.ndarray) -> float:
+    """rms distance (px) of the captured-mask edge from Bardeen's curve after the finite-distance
+    correction (``raytracing/boundary.py``: 1/8-px marching of the bilinear 0.5 level set)."""
+    from kerrray_b200.boundary import mask_centroid
+
+    cam = spec.camera
+    captured = state.reshape(cam.shape) == 2
+    alpha, beta = cam.pixel_coordinates()
+    c = mask_centroid(alpha, beta, captured)
+    edge = K.extract_boundary_from_mask(alpha, beta, captured, centre=c)
+    curve = K.analytic_boundary(spec.spacetime, cam.inclination_deg, 720)
+    err = K.boundary_error(edge, curve, c, pixel_size=cam.pixel_size,
+                           scale=K.finite_distance_scale(spec.spacetime, cam.radius))
+    return float(err["rms_px"])
+
+
+def sweep_edge_errors(K, specs, state: np.ndarray, offsets) -> dict:
+    """Per-image mask-edge rms against Bardeen (px), summarised per resolution."""
+    rows = []
+    for k, spec in enumerate(specs):
+        rows.append((spec.camera.resolution, edge_rms_px(K, spec, state[int(offsets[k]):int(offsets[k + 1])])))
+    out = {}
+    for res in sorted({r for r, _ in rows}):
+        v = [e for r, e in rows if r == res]
+        out[f"{res}^2"] = {"images": len(v), "median_px": float(np.median(v)), "max_px": float(np.max(v))}
+    return out
+
+
+def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024") -> dict:
+    """Mixed persistent + FP64 re-trace against the plain FP64 kernel on the a*=0.99, i=85 deg
+    image (rtol 1e-6): rays/s of each, whether the two shadow masks are identical, the terminal
+    states' difference and both masks' edge rms against Bardeen's curve."""
     import torch
 
-    specs = workload_specs(K, "spin99_1024")
+    specs = workload_specs(K, name)
     total = specs[0].n_rays
     tuned, _ = K.autotune(specs, precision="mixed", device=local)
     mixed = K.DeviceSweep(specs, precision="mixed", device=local,
@@ -275,12 +309,16 @@ def mixed_vs_plain(K, local: int, stream, flush) -> dict:
     differ = int((mixed.tensors["state"] != plain.tensors["state"]).sum().item())
     esc = (plain.tensors["state"] == 1) & (mixed.tensors["state"] == 1)
     rel = ((mixed.tensors["Y"] - plain.tensors["Y"]).abs() / plain.tensors["Y"].abs().clamp_min(1.0)).amax(dim=1)
-    out = {"workload": WORKLOADS["spin99_1024"], "photons": total,
+    st_plain = plain.tensors["state"].cpu().numpy()
+    st_mixed = mixed.tensors["state"].cpu().numpy()
+    out = {"workload": WORKLOADS[name], "photons": total,
            "mixed_retrace_rays_s": total / (t_mixed * 1e-3), "fast64_rays_s": total / (t_fast * 1e-3),
            "plain_fp64_rays_s": total / (t_plain * 1e-3), "speedup_mixed_vs_plain": t_plain / t_mixed,
            "mask_identical": same, "pixels_differing": differ, "retraced": int(ms["retraced"]),
            "escaped_max_rel_dY_vs_plain": float(rel[esc].max().item()),
            "escaped_median_rel_dY_vs_plain": float(rel[esc].median().item()),
+           "edge_rms_px_plain": edge_rms_px(K, specs[0], st_plain),
+           "edge_rms_px_mixed": edge_rms_px(K, specs[0], st_mixed),
            "mixed_launch": {"variant": tuned.variant, "refill_threshold": tuned.refill_threshold}}
     for sw in (mixed, fast, plain):
         sw.close()
@@ -360,7 +398,12 @@ def run_ours(args) -> None:
         plain.close()
         del plain
         torch.cuda.empty_cache()
-        extra["mixed_vs_plain_1024"] = mixed_vs_plain(K, local, stream, flush)
+        if args.workload == "sweep":
+            extra["edge_rms_px_vs_bardeen"] = sweep_edge_errors(K, specs, sweep.tensors["state"].cpu().numpy(),
+                                                                sweep.offsets)
+        extra["mixed_vs_plain_1024"] = mixed_vs_plain(K, local, stream, flush, "spin99_1024")
+        torch.cuda.empty_cache()
+        extra["mixed_vs_plain_2048"] = mixed_vs_plain(K, local, stream, flush, "spin99_2048")
         torch.cuda.empty_cache()
         # End to end through the public API: pinned host Y0 in, every result array out.
         y0 = torch.empty((total, 8), dtype=torch.float64, pin_memory=True).numpy()
@@ -418,6 +461,197 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def _line(metric: str, value: float, unit: str, args, ms_per_step: float, config: dict, **rest) -> dict:
+    return {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": config, **rest}
+
+
+def bisect_cases(K, rtols=(1e-6, 1e-8, 1e-10), n_angles: int = 1440, r_o: float = 1.0e5):
+    """The 36 cases (12 spacetimes/inclinations x 3 tolerances) of the batched edge bisection."""
+    angles = 2.0 * math.pi * np.arange(n_angles) / n_angles
+    cases = []
+    for rtol in rtols:
+        for spin in (0.0, 0.5, 0.9, 0.99):
+            for incl in (17.0, 60.0, 85.0):
+                cases.append(K.edge_study(K.Spacetime(1.0, spin), incl, r_o, rtol, angles, bracket=(2.0, 8.0)))
+    return cases
+
+
+def bisect_cpu_baseline(K, cases, target_s: float = 15.0) -> dict:
+    """The oracle (all host threads) on the first-halving rays (rho = 5 M) of a strided sample of
+    the bisection items: rays/s of the same integrations the bisection runs."""
+    from oracle import oracle as O
+
+    def run(stride: int):
+        n = 0
+        t0 = time.perf_counter()
+        for c in cases:
+            ang = c.angles[::stride]
+            rho = 0.5 * (c.r_lo[::stride] + c.r_hi[::stride])
+            a = c.centre[0] + rho * np.cos(ang)
+            b = c.centre[1] + rho * np.sin(ang)
+            integ, term = K.edge_options(c.rtol, c.r_o)
+            y0 = O.initial_states(1.0, c.spacetime.spin, c.r_o, c.inclination_deg, 0.0, a, b)
+            O.integrate(1.0, c.spacetime.spin, y0, O.Options(rtol=integ.rtol, atol=integ.atol, max_steps=integ.max_steps,
+                                                           lambda_max=integ.lambda_max, horizon_epsilon=1e-6,
+                                                           escape_radius=c.r_o))
+            n += ang.size
+        return n, time.perf_counter() - t0
+
+    stride = 1440
+    n, dt = run(stride)
+    while dt < 1.0 and stride > 1:
+        stride = max(1, stride // 8)
+        n, dt = run(stride)
+    reps = 1
+    if stride == 1 and dt < target_s:
+        reps = max(1, int(math.ceil(target_s / max(dt, 1e-3))))
+    else:
+        stride = max(1, int(stride * dt / target_s))
+    n = 0
+    dt = 0.0
+    for _ in range(reps):
+        n_k, dt_k = run(stride)
+        n += n_k
+        dt += dt_k
+    return {"value": n / dt, "unit": "rays/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"{n} first-halving rays (every {stride}th angle of each of the {len(cases)} cases, "
+                       f"{reps} pass(es)), {dt:.1f} s")}
+
+
+def run_bisect(args) -> None:
+    """Config 4: every item of every case in one persistent launch; the reference runs one
+    integrate_batch per halving (study_edge_bisection.py:53-68)."""
+    import torch
+
+    import kerrray_b200 as K
+    from kerrray_b200 import _lib
+
+    torch.cuda.set_device(0)
+    cases = bisect_cases(K)
+    n_items = sum(c.angles.size for c in cases)
+    iterations = 36
+    precision = "reference" if args.precision == "reference" else "fast64"
+    for _ in range(args.warmup):
+        K.bisect_edges(cases, 2, precision=precision)
+    with ClockSampler(0) as clocks:
+        kms, walls = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res, stats = K.bisect_edges(cases, iterations, precision=precision)
+            walls.append(time.perf_counter() - t0)
+            kms.append(stats["kernel_ms"])
+    rays = n_items * iterations
+    kernel_ms = statistics.mean(kms)
+    flops = algorithmic_flops({"attempts": stats["attempts"], "accepted": stats["accepted"], "photons": rays})
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    peak64 = _lib.fma_peak_tflops(0, True)
+    from kerrray_b200.bisect import edge_error
+
+    errors = {}
+    per_case = []
+    for c, (r_mid, width, fails) in zip(cases, res):
+        e = edge_error(c, r_mid)
+        per_case.append({"spin": c.spacetime.spin, "inclination_deg": c.inclination_deg, "rtol": c.rtol,
+                         "rms_M": e["rms_M"], "max_M": e["max_M"], "lost": int(fails)})
+        key = f"{c.rtol:g}"
+        d = errors.setdefault(key, {"rms_M": [], "max_M": [], "lost": 0, "max_width_M": 0.0})
+        d["rms_M"].append(e["rms_M"])
+        d["max_M"].append(e["max_M"])
+        d["lost"] += int(fails)
+        d["max_width_M"] = max(d["max_width_M"], float(np.max(width)))
+    summary = {k: {"rms_M_median": float(np.median(v["rms_M"])), "rms_M_max": float(np.max(v["rms_M"])),
+                   "max_M": float(np.max(v["max_M"])), "rms_over_rtol_median": float(np.median(v["rms_M"])) / float(k),
+                   "lost": v["lost"], "max_width_M": v["max_width_M"]} for k, v in errors.items()}
+    cpu = None if args.no_cpu else bisect_cpu_baseline(K, cases)
+    line = _line("edge-bisection rays/s per B200 (batched, one persistent launch)", rays / (kernel_ms * 1e-3),
+                 "rays/s", args, kernel_ms,
+                 {"workload": WORKLOADS["bisect"], "items": n_items, "iterations": iterations, "cases": len(cases),
+                  "precision": precision, "kernel": "k_bisect_edges (one item per lane, all halvings in registers)",
+                  "l2": "inputs < 1 MB; the work is FP64 arithmetic in registers"},
+                 e2e={"value": rays / statistics.mean(walls), "unit": "rays/s", "h2d_bytes_per_step": n_items * 36,
+                      "d2h_bytes_per_step": n_items * 24},
+                 gpu_launches=args.steps,
+                 roofline={"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                           "frac": achieved / peak64, "traffic": None,
+                           "peak_source": "measured FP64 FMA chains on this device (krr_fma_peak)"},
+                 cpu_baseline=cpu, clocks=clocks.summary(), edge_error_vs_bardeen=summary,
+                 worst_cases=sorted(per_case, key=lambda d: -d["max_M"])[:6],
+                 queue={"attempts": stats["attempts"], "accepted": stats["accepted"],
+                        "lane_occupancy": stats["busy_slots"] / max(stats["lane_slots"], 1)})
+    print(json.dumps(line), flush=True)
+
+
+def run_lensing(args) -> None:
+    """Config 5: forward pass with tape + reverse sweep for ~50k rays; FD check on a sample;
+    Gauss-Newton fit of (a*, i) from (0.5, 50 deg) to the map at (0.8, 60 deg)."""
+    import torch
+
+    import kerrray_b200 as K
+    from kerrray_b200 import _lib
+
+    torch.cuda.set_device(0)
+    alpha, beta = K.edge_distant_rays(0.8, 60.0)
+    n = alpha.numel()
+    stream = torch.cuda.current_stream(0)
+    for _ in range(args.warmup):
+        res = K.lensing_map(alpha, beta, 0.8, 60.0)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        ms = []
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = K.lensing_map(alpha, beta, 0.8, 60.0)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    kernel_ms = statistics.mean(ms)
+    ok = int(((res.status == 0) & (res.state == 1)).sum().item())
+    steps = res.n_steps.double()
+    # FD of the recorded map on a strided sample of 1024 rays (h = 1e-6).
+    from kerrray_b200 import adjoint as A
+
+    idx = torch.arange(0, n, max(1, n // 1024), device=alpha.device)[:1024]
+    sub = A.lensing_map(alpha[idx], beta[idx], 0.8, 60.0)
+    h = 1e-6
+    fd = np.zeros((idx.numel(), 2, 4))
+    for p_ in range(4):
+        outs = []
+        for sgn in (1.0, -1.0):
+            d = [0.0] * 4
+            d[p_] = sgn * h
+            th, ph = A.replay(sub, alpha[idx] + d[0], beta[idx] + d[1], 0.8 + d[2], 60.0 + d[3])
+            outs.append(np.stack([th.cpu().numpy(), ph.cpu().numpy()], axis=1))
+        fd[:, :, p_] = (outs[0] - outs[1]) / (2 * h)
+    jac = sub.jac.cpu().numpy()
+    err = np.abs(jac - fd) / np.maximum(np.abs(fd), np.sqrt(np.mean(fd**2, axis=0, keepdims=True)))
+    t0 = time.perf_counter()
+    fit = K.fit_spin_inclination(alpha, beta, res.theta, res.phi, p0=(0.5, 50.0), iterations=20)
+    torch.cuda.synchronize()
+    fit_s = time.perf_counter() - t0
+    mag = K.magnification(res.jac)
+    line = _line("lensing-map adjoint rays/s per B200 (forward with tape + reverse sweep, 4 parameters)",
+                 n / (kernel_ms * 1e-3), "rays/s", args, kernel_ms,
+                 {"workload": WORKLOADS["lensing"], "rays": n, "checkpoint_every": 32,
+                  "kernel": "k_lensing_adjoint (one ray per thread)",
+                  "l2": "tape of accepted step sizes in HBM (n x 8192 x 8 B), written once and read once"},
+                 e2e=None, gpu_launches=args.steps,
+                 roofline=None, cpu_baseline=None, clocks=clocks.summary(),
+                 rays_ok=ok, accepted_steps={"mean": float(steps.mean().item()), "max": int(steps.max().item())},
+                 fd_check={"rays": int(idx.numel()), "h": h, "max_rel": float(err.max()),
+                           "median_rel": float(np.median(err)),
+                           "metric": "|J - FD| / max(|FD|, column RMS), FD of the recorded map"},
+                 gauss_newton={"start": [0.5, 50.0], "target": [0.8, 60.0], "spin": fit["spin"],
+                               "inclination_deg": fit["inclination_deg"], "iterations": len(fit["history"]) - 1,
+                               "map_evaluations": fit["evaluations"],
+                               "final_cost": fit["history"][-1]["cost"], "seconds": fit_s},
+                 magnification={"median": float(mag.median().item()), "max": float(mag.max().item())})
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,6 +667,10 @@ def main() -> None:
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "bisect":
+        run_bisect(args)
+    elif args.workload == "lensing":
+        run_lensing(args)
     else:
         run_ours(args)
 

@@ -6,6 +6,14 @@ C++ behind the C ABI of ``include/kerrray_cuda.h``); this package is the host si
 """
 
 from kerrray_b200._lib import BackendUnavailable
+from kerrray_b200.adjoint import (
+    LensingFunction,
+    LensingResult,
+    edge_distant_rays,
+    fit_spin_inclination,
+    lensing_map,
+    magnification,
+)
 from kerrray_b200.autotune import autotune, list_variants
 from kerrray_b200.backends import (
     BACKEND_NAMES,
@@ -30,6 +38,15 @@ from kerrray_b200.orbits import critical_impact_parameters, shadow_curve
 from kerrray_b200.rays import concatenate_results, trace_rays
 from kerrray_b200.shadow import FAILURE_STATES, ShadowImage, compute_shadow, shadow_mask_int8, state_counts
 from kerrray_b200.sweep import DeviceSweep, ImageSpec, LaunchConfig, SweepResult, order_by_cost, trace_images
+from kerrray_b200.validation import (
+    critical_impacts,
+    equatorial_photon,
+    photon_from_constants,
+    photon_sphere,
+    tangential_photon,
+    winding_rate_prediction,
+    winding_rates,
+)
 from kerrray_b200.types import (
     BatchResult,
     EventOptions,
@@ -42,6 +59,9 @@ from kerrray_b200.types import (
 )
 
 __all__ = [
+    "LensingFunction", "LensingResult", "edge_distant_rays", "fit_spin_inclination", "lensing_map", "magnification",
+    "critical_impacts", "equatorial_photon", "photon_from_constants", "photon_sphere", "tangential_photon",
+    "winding_rate_prediction", "winding_rates",
     "EdgeCase", "analytic_boundary", "bisect_edge", "bisect_edges", "boundary_error", "critical_impact_parameters",
     "edge_options", "edge_study", "extract_boundary_from_mask", "finite_distance_scale", "polygon_centroid",
     "polygon_radii", "shadow_curve", "summarise_shadow",

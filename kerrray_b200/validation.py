@@ -10,7 +10,11 @@ argument:
   above, ``n_probe`` interior probes per iteration;
 * :func:`critical_impacts` -- bracketing of the capture threshold in impact parameter for
   inward equatorial rays (``src/kerrray/validation/kerr_bisection.py:96-263``), prograde and
-  retrograde searches sharing one batch per iteration.
+  retrograde searches sharing one batch per iteration;
+* :func:`winding_rate_prediction`, :func:`winding_rates` -- the near-critical winding study
+  (``scripts/study_winding.py:73-127``): turns of equatorial photons launched at
+  ``b = b_c (1 + delta)`` against ``log10(delta)``, compared with the orbit's instability rate
+  ``ln(10) / (2 pi gamma_phi)``; all deltas and both directions of one spin in one batch.
 """
 
 from __future__ import annotations
@@ -23,8 +27,9 @@ import numpy as np
 
 from kerrray_b200.types import Spacetime, TerminationState, outer_horizon
 
-__all__ = ["CRITICAL_IMPACT_REFERENCE", "PHOTON_SPHERE_REFERENCE", "critical_impacts", "photon_from_constants",
-           "photon_sphere", "tangential_photon"]
+__all__ = ["CRITICAL_IMPACT_REFERENCE", "PHOTON_SPHERE_REFERENCE", "WINDING_DELTAS", "WINDING_SPINS", "critical_impacts",
+           "equatorial_photon", "photon_from_constants", "photon_sphere", "tangential_photon", "winding_rate_prediction",
+           "winding_rates"]
 
 PHOTON_SPHERE_REFERENCE = 3.0                   # r_ph = 3M (a = 0)
 CRITICAL_IMPACT_REFERENCE = 3.0 * math.sqrt(3.0)  # b_c = 3 sqrt(3) M (a = 0)
@@ -65,6 +70,16 @@ def photon_from_constants(st, r: float, theta: float, E: float, Lz: float, Q: fl
 
 def _lz_sign(st, prograde: bool) -> float:
     return 1.0 if prograde == (st.a >= 0.0) else -1.0
+
+
+def equatorial_photon(st, r0: float, b: float, *, inward: bool = True, prograde: bool = True,
+                      E: float = 1.0) -> np.ndarray:
+    """Equatorial photon at ``r0`` with impact parameter ``b = |L_z| / E``, ``Q = 0``
+    (``geodesics/initial_conditions.py:121-141``)."""
+    if b < 0.0:
+        raise ValueError(f"b must be >= 0, got {b!r}")
+    return photon_from_constants(st, r0, 0.5 * math.pi, E, _lz_sign(st, prograde) * b * E, 0.0,
+                                 sign_r=-1 if inward else 1, sign_theta=1)
 
 
 def tangential_photon(st, r0: float, *, prograde: bool = True, E: float = 1.0) -> np.ndarray:
@@ -210,3 +225,76 @@ def critical_impacts(st, integ, term, *, r0: float, b_lo: float, b_hi: float, to
     runtime = time.perf_counter() - t0
     return tuple(CriticalImpactResult(st.spin, p, 0.5 * (lo[p] + hi[p]), lo[p], hi[p], hi[p] - lo[p], its[p], n_rays,
                                       max_steps, runtime) for p in directions)
+
+
+WINDING_SPINS = (0.0, 0.3, 0.6, 0.9, 0.99)
+WINDING_DELTAS = (1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8)
+
+
+def winding_rate_prediction(spin: float, prograde: bool, mass: float = 1.0) -> float:
+    """Turns per decade of ``b / b_c - 1``, ``ln(10) / (2 pi gamma_phi)``, for the circular
+    equatorial photon orbit (``study_winding.py:66-83``; Carter 1968, Bardeen, Press & Teukolsky
+    1972). With ``E = 1``, ``theta = pi/2`` and signed ``xi = L_z / E`` (positive for prograde at
+    ``a >= 0``), ``R(r) = (r^2 + a^2 - a xi)^2 - Delta (xi - a)^2`` and
+    ``Phi(r) = (xi - a) + (a / Delta)(r^2 + a^2 - a xi)``; ``gamma_phi = sqrt(R''(r_ph)/2)/|Phi(r_ph)|``.
+    ``R''`` is taken in closed form, ``8 r^2 + 4 (r^2 + a^2 - a xi) - 2 (xi - a)^2`` (with
+    ``u = r^2 + a^2 - a xi``: ``(u^2)'' = 2 u'^2 + 2 u u''``, ``u' = 2 r``, ``u'' = 2``,
+    ``Delta'' = 2``); the study takes it by central differences of ``R``."""
+    from kerrray_b200.orbits import critical_impact_parameters, equatorial_photon_orbit_radius
+
+    st = Spacetime(mass, spin)
+    a = st.a
+    r_ph = equatorial_photon_orbit_radius(st, prograde=prograde)
+    b_pro, b_retro = critical_impact_parameters(st)
+    xi = b_pro if prograde else -b_retro
+    u = r_ph * r_ph + a * a - a * xi
+    r2 = 8.0 * r_ph * r_ph + 4.0 * u - 2.0 * (xi - a) ** 2
+    delta = r_ph * r_ph - 2.0 * mass * r_ph + a * a
+    phi_rate = (xi - a) + a / delta * u
+    gamma = math.sqrt(r2 / 2.0) / abs(phi_rate)
+    return math.log(10.0) / (2.0 * math.pi * gamma)
+
+
+@dataclass
+class WindingResult:
+    spin: float
+    prograde: bool
+    b_c: float
+    turns: np.ndarray          # per delta
+    states: np.ndarray         # termination codes per delta
+    rate_per_decade: float     # -slope of turns against log10(delta) over the escaped rays
+    predicted: float
+    relative_difference: float
+
+
+def winding_rates(spins=WINDING_SPINS, deltas=WINDING_DELTAS, *, rtol: float = 1e-12, r0: float = 50.0,
+                  escape_radius: float = 60.0, max_steps: int = 400_000, backend=None) -> list[WindingResult]:
+    """Measured against predicted winding rates (``study_winding.py:86-99``, ``:108-114``): the
+    nine cases of the study by default (spin 0 has one direction), ``rk45`` at ``rtol`` with
+    ``atol = 1e-2 rtol``, launch radius 50 M, escape radius 60 M, horizon margin 1e-6."""
+    from kerrray_b200.orbits import critical_impact_parameters
+    from kerrray_b200.types import IntegratorOptions, TerminationOptions
+
+    engine = _backend(backend)
+    integ = IntegratorOptions(method="rk45", rtol=rtol, atol=rtol * 1e-2, max_steps=max_steps)
+    term = TerminationOptions(horizon_epsilon=1e-6, escape_radius=escape_radius)
+    deltas = np.asarray(deltas, dtype=np.float64)
+    out = []
+    for spin in spins:
+        st = Spacetime(1.0, spin)
+        directions = (True,) if spin == 0.0 else (True, False)
+        b_pro, b_retro = critical_impact_parameters(st)
+        y0 = np.stack([equatorial_photon(st, r0, (b_pro if p else b_retro) * (1.0 + d), prograde=p)
+                       for p in directions for d in deltas])
+        res = engine.integrate_batch(st, y0, integ, term)
+        turns_all = np.abs(np.asarray(res.Y)[:, 3] - y0[:, 3]) / (2.0 * math.pi)
+        for k, p in enumerate(directions):
+            sl = slice(k * deltas.size, (k + 1) * deltas.size)
+            turns, states = turns_all[sl], np.asarray(res.state)[sl]
+            ok = states == TerminationState.ESCAPED
+            rate = float("nan")
+            if ok.sum() >= 3:
+                rate = -float(np.polyfit(np.log10(deltas[ok]), turns[ok], 1)[0])
+            pred = winding_rate_prediction(spin, p)
+            out.append(WindingResult(spin, p, b_pro if p else b_retro, turns, states, rate, pred, (rate - pred) / pred))
+    return out

@@ -300,6 +300,49 @@ def main() -> None:
     term_v = TerminationOptions()
     tang = np.stack([tangential_photon(st0, r) for r in (2.5, 2.9, 3.0 + 1e-3, 3.1, 4.0)])
     _run("tangential_photons_a0", st0, tang, integ_v, term_v)
+
+    # 15. Near-critical winding (scripts/study_winding.py:73-127): the reference's own predicted
+    #     rate and its scalar-integrator measurement for the nine (spin, direction) cases, plus the
+    #     numba backend on the same initial states (the batch path the cuda backend replaces).
+    #     The study imports matplotlib only for its figure; an inert stub stands in for it here.
+    import types
+
+    for name in ("matplotlib", "matplotlib.pyplot"):
+        stub = types.ModuleType(name)
+        stub.use = lambda *a, **k: None
+        sys.modules.setdefault(name, stub)
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    import study_winding  # noqa: E402
+    from kerrray.geodesics.initial_conditions import equatorial_photon  # noqa: E402
+
+    deltas = [1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8]
+    cases = [(s, p) for s in (0.0, 0.3, 0.6, 0.9, 0.99) for p in (True, False) if not (s == 0.0 and not p)]
+    wind = {"deltas": np.array(deltas), "spins": np.array([c[0] for c in cases]),
+            "prograde": np.array([c[1] for c in cases])}
+    pred, rate, turns, b_cs, y0s, ys, states, steps = [], [], [], [], [], [], [], []
+    integ_w = IntegratorOptions(method="rk45", rtol=1e-12, atol=1e-14, max_steps=400_000)
+    term_w = TerminationOptions(horizon_epsilon=1e-6, escape_radius=60.0)
+    with np.errstate(all="ignore"):
+        for spin, prograde in cases:
+            gamma, _, _ = study_winding.predicted_gamma(spin, prograde)
+            pred.append(math.log(10) / (2 * math.pi * gamma))
+            m = study_winding.measured_rate(spin, prograde, deltas)
+            rate.append(m["rate_per_decade"])
+            turns.append(m["turns"])
+            b_cs.append(m["b_c"])
+            stw = Spacetime(1.0, spin)
+            y0 = np.stack([equatorial_photon(stw, 50.0, m["b_c"] * (1 + d), prograde=prograde) for d in deltas])
+            res = BACKEND.integrate_batch(stw, y0, integ_w, term_w)
+            y0s.append(y0)
+            ys.append(res.Y)
+            states.append(res.state)
+            steps.append(res.n_steps)
+    wind.update(predicted=np.array(pred), rate_scalar=np.array(rate), turns_scalar=np.array(turns),
+                b_c=np.array(b_cs), Y0=np.array(y0s), Y=np.array(ys), state=np.array(states), n_steps=np.array(steps))
+    np.savez_compressed(OUT / "winding.npz", **wind)
+    for (spin, prograde), p, r in zip(cases, pred, rate):
+        print(f"winding a={spin} {'pro' if prograde else 'retro'}: predicted {p:.5f} measured {r:.5f} "
+              f"({100 * (r - p) / p:+.3f}%)")
     print(f"done in {time.perf_counter() - t0:.1f} s")
 
 

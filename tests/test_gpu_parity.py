@@ -361,6 +361,31 @@ def test_exact_checks_on_the_cuda_backend() -> None:
     assert abs(pro.b_c - b_pro) < 1e-5 and abs(retro.b_c - b_retro) < 1e-5
 
 
+def test_winding_rates_on_the_cuda_backend() -> None:
+    """The near-critical winding study (nine spin/direction cases, deltas 1e-3..1e-8, rtol 1e-12)
+    on the cuda backend: turns against the reference's numba backend on the same rays, and the
+    measured rate against the orbit's instability rate (the reference: within 0.04 %)."""
+    from kerrray_b200 import validation as V
+
+    d = golden("winding")
+    rows = V.winding_rates()
+    assert len(rows) == 9
+    worst = 0.0
+    for k, row in enumerate(rows):
+        assert row.spin == d["spins"][k] and row.prograde == d["prograde"][k]
+        assert np.all(row.states == 1)
+        turns_ref = np.abs(d["Y"][k][:, 3] - d["Y0"][k][:, 3]) / (2 * np.pi)
+        # Last-bit differences of CUDA's sin/cos flip a few accept/reject decisions at rtol 1e-12;
+        # near the orbit they grow with the winding (up to ~20 turns at a* = 0.99). The reference's
+        # own scalar integrator and numba backend differ by 1.4e-4 turns on these rays.
+        assert np.abs(row.turns - turns_ref).max() < 1e-4, (row.spin, row.prograde, row.turns - turns_ref)
+        rate_ref = -np.polyfit(np.log10(d["deltas"]), turns_ref, 1)[0]
+        assert abs(row.rate_per_decade - rate_ref) <= 2e-5 * rate_ref
+        worst = max(worst, abs(row.relative_difference))
+    print("winding: worst |measured - predicted| / predicted", worst)
+    assert worst < 5e-4
+
+
 def _lens_rays(n_side: int = 16, fov: float = 12.0, min_r: float = 7.0):
     torch = pytest.importorskip("torch")
     c = fov * (2.0 * np.arange(n_side) + 1.0 - n_side) / n_side
@@ -474,3 +499,16 @@ def test_autograd_function_and_gauss_newton_fit() -> None:
     fit = A.fit_spin_inclination(alpha, beta, target.theta, target.phi, p0=(0.5, 50.0), iterations=20)
     print("Gauss-Newton:", fit["spin"], fit["inclination_deg"], fit["history"][-1])
     assert abs(fit["spin"] - 0.8) < 1e-6 and abs(fit["inclination_deg"] - 60.0) < 1e-5
+
+
+def test_gauss_newton_fit_on_edge_distant_rays() -> None:
+    """The lensing fit on an image's escaped rays more than 3 px from the shadow edge (the
+    strongly lensed rays included): (0.5, 50 deg) -> (0.8, 60 deg) within 20 iterations."""
+    from kerrray_b200 import adjoint as A
+
+    alpha, beta = A.edge_distant_rays(0.8, 60.0, resolution=128)
+    assert alpha.numel() > 10000
+    target = A.lensing_map(alpha, beta, 0.8, 60.0)
+    fit = A.fit_spin_inclination(alpha, beta, target.theta, target.phi, p0=(0.5, 50.0), iterations=20)
+    print("edge-distant fit:", alpha.numel(), "rays", fit["spin"], fit["inclination_deg"], fit["evaluations"], "maps")
+    assert abs(fit["spin"] - 0.8) < 1e-8 and abs(fit["inclination_deg"] - 60.0) < 1e-6

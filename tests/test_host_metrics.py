@@ -46,3 +46,18 @@ def test_mask_edge_extraction_and_error_match_reference() -> None:
     for k, v in ref.items():
         assert abs(err[k] - v) <= 1e-9 * max(1.0, abs(v)), k
     assert err["rms_px"] < 0.5  # the mask edge within half a pixel of Bardeen's curve
+
+
+def test_winding_prediction_and_initial_states_match_reference() -> None:
+    """Closed-form R'' against the study's central differences; equatorial photon states."""
+    from kerrray_b200 import validation as V
+    from kerrray_b200.types import Spacetime
+
+    d = golden("winding")
+    for k, (spin, prograde) in enumerate(zip(d["spins"], d["prograde"])):
+        pred = V.winding_rate_prediction(float(spin), bool(prograde))
+        assert abs(pred - d["predicted"][k]) <= 1e-7 * pred
+        st = Spacetime(1.0, float(spin))
+        for j, delta in enumerate(d["deltas"]):
+            y = V.equatorial_photon(st, 50.0, float(d["b_c"][k]) * (1 + float(delta)), prograde=bool(prograde))
+            assert np.allclose(y, d["Y0"][k][j], rtol=1e-14, atol=0.0)

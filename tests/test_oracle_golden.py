@@ -69,3 +69,14 @@ def test_flop_count_per_attempt_is_constant() -> None:
     assert per_attempt == {"add": 377.0, "mul": 702.0, "div": 111.0, "sqrt": 1.0, "trig": 18.0, "pow": 1.0}
     assert sum(c["accept"].values()) == 28 * c["accepted"]
     assert sum(c["init"].values()) == 127 * c["rays"]
+
+
+def test_oracle_winding_rays_match_reference() -> None:
+    """The winding study's 54 near-critical equatorial rays (rtol 1e-12, escape radius 60 M)."""
+    d = golden("winding")
+    opts = O.Options(rtol=1e-12, atol=1e-14, max_steps=400_000, escape_radius=60.0)
+    for k, spin in enumerate(d["spins"]):
+        out = O.integrate(1.0, float(spin), d["Y0"][k], opts)
+        assert np.array_equal(out["state"], d["state"][k].astype(np.int64))
+        assert np.array_equal(out["n_steps"], d["n_steps"][k].astype(np.int64))
+        assert np.array_equal(out["Y"], d["Y"][k])
