@@ -265,7 +265,7 @@ KRR_API int krr_lensing_replay(int device, const krr_lens_params* params, const 
  * device-memory budget, work enqueued on a stream another library captures, a plug-in whose
  * host owns all device memory): the launch's scratch (work-queue counters and image
  * descriptors) lives in a static array in the library's device image, sized for at most
- * KRR_NOALLOC_MAX_IMAGES images (about 47 KB per device, held until exit); larger batches are
+ * KRR_NOALLOC_MAX_IMAGES images (about 46 KB per device, held until exit); larger batches are
  * rejected with KRR_ERR_INVALID.  Inputs (d_Y0, nullable) and outputs (d_out) are the caller's
  * device buffers; nothing is allocated.  The first call on a device looks up the array's
  * device address, so make that first call before any stream capture.  All calls share the

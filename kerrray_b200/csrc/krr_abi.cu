@@ -105,10 +105,8 @@ krr::Params make_params(double mass, double spin, const krr_options* o) {
   P.disk = o->disk_plane != 0;
   P.r_plus = outer_horizon(m, a);
   P.f_mass = (float)m;
+  P.f_a = (float)P.a;
   P.f_a2 = (float)P.a2;
-  P.f_neg_2ma = (float)P.neg_2ma;
-  P.f_pos_2ma = (float)P.pos_2ma;
-  P.f_two_a2 = (float)P.two_a2;
   P.f_rpm = (float)(2.0 * std::sqrt(m * m - a * a));
   return P;
 }

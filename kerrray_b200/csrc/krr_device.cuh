@@ -74,15 +74,24 @@ struct Params {
   int rk4;   // 0: Dormand-Prince 5(4), 1: fixed-step RK4
   int disk;  // disk-plane event enabled
   // FP32 copies for the mixed mode's stages (rounded once on the host).
-  float f_mass, f_a2, f_neg_2ma, f_pos_2ma, f_two_a2;
+  float f_mass, f_a, f_a2;
   float f_rpm;  // r_plus - r_minus = 2 sqrt(M^2 - a^2)
 };
 
 // Per-ray conservation references (numba_backend.py:174-178).  E and L_z are exact constants
-// of the integration here, so only Q0 and the floors are kept.
+// of the integration here, so only Q0 and the two denominators of the drifts are kept:
+// max(|Q0|, E0^2 M^2) for the Carter constant and E0^2 for the null error.  The reference
+// modes divide by them; the fast modes keep their reciprocals and multiply.
 struct Refs {
-  double q0, fq, fe2;
+  double q0, q_den, e_den;
 };
+
+// x / den in the reference modes, x * den (den holding the reciprocal) in the fast modes.
+template <class M>
+__device__ __forceinline__ double drift(double x, double den) {
+  if constexpr (M::kFused) return x * den;
+  else return x / den;
+}
 
 // ------------------------------------------------------------------------------------------
 // Arithmetic modes.
@@ -129,7 +138,6 @@ struct RefMode {
   using S = W;  // state type
   using K = W;  // stage type
   using N = W;  // error-norm type
-  static constexpr bool kFastFactor = false;
   static constexpr bool kFused = false;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
@@ -218,12 +226,80 @@ struct RefMode {
   }
 };
 
-// FP64 with contraction, sincos and reciprocals.  Same closed forms as RefMode, rearranged.
+// ------------------------------------------------------------------------------------------
+// The fast modes' right-hand side: the same Hamiltonian in Carter's separated form,
+//
+//   2 Sigma H = Delta p_r^2 + p_theta^2 - K^2 / Delta + v^2,
+//   K = (r^2 + a^2) E - a L,   v = L / sin(theta) - a E sin(theta),   E = -p_t,   L = p_phi,
+//
+// which is an algebraic identity of g^{mu nu} p_mu p_nu for the Boyer-Lindquist inverse metric
+// (Carter 1968, Phys. Rev. 174, 1559).  Hamilton's equations of this form are therefore the
+// reference's right-hand side (numba_kernel.py:158-197) on and off the null shell; only the
+// rounding differs.  They take about 50 operations and three reciprocals, where the fifteen
+// metric terms and their derivatives take about 95 operations and seventeen divisions.  For
+// L = 0 the 1/sin terms vanish identically, as the reference's polar-axis guard makes them.
+// ------------------------------------------------------------------------------------------
+
+// 1/x by Newton-Raphson on the hardware's approximate FP64 reciprocal: r <- r + r (1 - x r)
+// converges quadratically (steps = 1: about 46 correct bits; steps = 2: a rounding error).
+// A zero, infinite or subnormal x gives NaN, where a division gives an infinity: either way the
+// step is non-finite and the ray a NUMERICAL_FAILURE.
+template <int STEPS = 2>
+__device__ __forceinline__ double rcp_newton(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+#pragma unroll
+  for (int i = 0; i < STEPS; ++i) r = fma(r, fma(-x, r, 1.0), r);
+  return r;
+}
+__device__ __forceinline__ double rcp_fast(double x) { return rcp_newton<2>(x); }
+__device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
+
+// Per-ray constants of the separated form.
+template <class T>
+struct Motion {
+  T e, l;    // E = -p_t, L = p_phi
+  T ae, al;  // a E, a L
+  T m2e;     // -2 E
+  __device__ void set(T pt, T pph, T a) {
+    e = -pt;
+    l = pph;
+    ae = a * e;
+    al = a * l;
+    m2e = T(-2) * e;
+  }
+};
+
+// f (six integrated components) at (r, theta, p_r, p_theta) with Delta supplied by the mode.
+template <class T>
+__device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth, const Motion<T>& mo, T a, T a2,
+                                              T m, T f[NV]) {
+  const T r2 = r * r;
+  const T r2a2 = r2 + a2;
+  const T k = fused(r2a2, mo.e, -mo.al);                    // K
+  const T isig = rcp_fast(fused(a2, c * c, r2));           // 1 / Sigma
+  const T kd = k * rcp_fast(dlt);                          // K / Delta
+  const T is = (mo.l != T(0)) ? rcp_fast(s) : T(0);        // 1 / sin (unused for L = 0)
+  const T lis = mo.l * is;                                 // L / sin
+  const T v = fused(-mo.ae, s, lis);                       // L / sin - a E sin
+  const T rm = r - m;
+  const T pr2 = pr * pr;
+  const T bs = fused(v, v, fused(dlt, pr2, pth * pth) - k * kd) * isig;  // 2 H = B / Sigma
+  f[CT] = isig * fused(a * s, v, kd * r2a2);               // -dH/dE
+  f[CR] = dlt * pr * isig;                                 // dH/dp_r
+  f[CTH] = pth * isig;                                     // dH/dp_theta
+  f[CPH] = isig * fused(a, kd, fused(lis, is, -mo.ae));    // dH/dL = (a K / Delta + L / sin^2 - a E) / Sigma
+  // -dH/dr = (r B / Sigma - (r - M) p_r^2 - (K / Delta)((K / Delta)(r - M) - 2 E r)) / Sigma
+  f[CPR] = isig * fused(r, bs, -fused(rm, pr2, kd * fused(kd, rm, mo.m2e * r)));
+  // -dH/dtheta = cos (v (L / sin^2 + a E) - a^2 sin B / Sigma) / Sigma
+  f[CPTH] = (isig * c) * fused(v, fused(lis, is, mo.ae), -(a2 * s) * bs);
+}
+
+// FP64 with explicit FMAs, sincos and Newton reciprocals on the separated form.
 struct Fast64 {
   using S = double;
   using K = double;
   using N = double;
-  static constexpr bool kFastFactor = true;
   static constexpr bool kFused = true;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
@@ -250,57 +326,13 @@ struct Fast64 {
 
   __device__ static void rhs(const Params& P, double r, double th, double pt, double pr, double pth, double pph,
                              double f[NV], Trig& tr) {
-    const double m = P.mass, a2 = P.a2;
     double s, c;
     sincos(th, &s, &c);
     tr.s = s;
     tr.c = c;
-    const double s2 = s * s;
-    const double sin2th = 2.0 * s * c;
-    const double r2 = r * r;
-    const double sig = fma(a2, c * c, r2);
-    const double dlt = fma(r, r - P.two_m, a2);
-    const double r2a2 = r2 + a2;
-    const double big_a = fma(r2a2, r2a2, -a2 * dlt * s2);
-    const double isig = 1.0 / sig;
-    const double idlt = 1.0 / dlt;
-    const double isd = isig * idlt;
-    const double isd2 = isd * isd;
-    const double isig2 = isig * isig;
-    const double sd = sig * dlt;
-    const double sig_r = 2.0 * r;
-    const double sig_th = -a2 * sin2th;
-    const double dlt_r = 2.0 * (r - m);
-    const double a_r = fma(4.0 * r, r2a2, -P.two_a2 * (r - m) * s2);
-    const double a_th = -a2 * dlt * sin2th;
-    const double sd_r = fma(sig_r, dlt, sig * dlt_r);
-    const double sd_th = sig_th * dlt;
-    const double g0 = -big_a * isd;
-    const double g1 = P.neg_2ma * r * isd;
-    const double g2 = dlt * isig;
-    const double g3 = isig;
-    const double g5 = fma(big_a, sd_r, -a_r * sd) * isd2;
-    const double g6 = P.neg_2ma * fma(-r, sd_r, sd) * isd2;
-    const double g7 = fma(dlt_r, sig, -dlt * sig_r) * isig2;
-    const double g8 = -sig_r * isig2;
-    const double g10 = fma(big_a, sd_th, -a_th * sd) * isd2;
-    const double g11 = P.pos_2ma * r * sd_th * isd2;
-    const double g12 = -dlt * sig_th * isig2;
-    const double g13 = -sig_th * isig2;
-    double g4 = 0.0, g9 = 0.0, g14 = 0.0;
-    if (pph != 0.0) {  // polar-axis guard
-      const double is2 = 1.0 / s2;
-      g4 = fma(-a2, s2, dlt) * isd * is2;
-      g9 = fma(-sig_r * isig2, is2, a2 * sd_r * isd2);
-      g14 = fma(-fma(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
-    }
-    f[CT] = fma(g0, pt, g1 * pph);
-    f[CR] = g2 * pr;
-    f[CTH] = g3 * pth;
-    f[CPH] = fma(g1, pt, g4 * pph);
-    const double pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
-    f[CPR] = -0.5 * fma(g5, pt2, fma(2.0 * g6, ptpph, fma(g7, pr2, fma(g8, pth2, g9 * pph2))));
-    f[CPTH] = -0.5 * fma(g10, pt2, fma(2.0 * g11, ptpph, fma(g12, pr2, fma(g13, pth2, g14 * pph2))));
+    Motion<double> mo;
+    mo.set(pt, pph, P.a);
+    rhs_separated<double>(fma(r, r - P.two_m, P.a2), r, s, c, pr, pth, mo, P.a, P.a2, P.mass, f);
   }
 };
 
@@ -312,12 +344,13 @@ struct Mixed {
   using S = double;
   using K = float;
   using N = double;
-  static constexpr bool kFastFactor = true;
   static constexpr bool kFused = true;
 
-  // FP32 copy of what the stages read: r - r_plus, r, theta, p_r, p_theta and the constants.
+  // FP32 copy of what the stages read: r - r_plus, r, theta, p_r, p_theta, and the ray's
+  // constants of motion.
   struct Shadow {
-    float d0, r, th, pr, pth, pt, pph;
+    float d0, r, th, pr, pth;
+    Motion<float> mo;
   };
 
   // The accepted state's diagnostics (Carter constant, axis test) use FP64 sine and cosine.
@@ -336,10 +369,9 @@ struct Mixed {
   }
 
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow& sh, K f[NV], Trig& tr) {
-    sh.pt = (float)pt;
-    sh.pph = (float)pph;
+    sh.mo.set((float)pt, (float)pph, (float)P.a);
     accepted(P, y, sh);
-    rhs_f(P, sh.d0, sh.r, sh.th, sh.pt, sh.pr, sh.pth, sh.pph, f, tr);
+    rhs_f(P, sh.d0, sh.r, sh.th, sh.pr, sh.pth, sh.mo, f, tr);
   }
 
   template <bool LAST, class R>
@@ -349,67 +381,20 @@ struct Mixed {
       for (int i = 0; i < NV; ++i) yn[i] = ry.y[i] + (double)(h * acc[i]);  // FP64 accumulation
     }
     const Shadow& sh = ry.sh;
-    rhs_f(P, fmaf(h, acc[CR], sh.d0), fmaf(h, acc[CR], sh.r), fmaf(h, acc[CTH], sh.th), sh.pt,
-          fmaf(h, acc[CPR], sh.pr), fmaf(h, acc[CPTH], sh.pth), sh.pph, f, tr);
+    rhs_f(P, fmaf(h, acc[CR], sh.d0), fmaf(h, acc[CR], sh.r), fmaf(h, acc[CTH], sh.th), fmaf(h, acc[CPR], sh.pr),
+          fmaf(h, acc[CPTH], sh.pth), sh.mo, f, tr);
   }
 
-  // The right-hand side in FP32 at (r - r_plus = d, r, theta, p).
-  __device__ static void rhs_f(const Params& P, float d, float rf, float thf, float pt, float pr, float pth,
-                               float pph, float f[NV], Trig& tr) {
-    const float dlt = d * (d + P.f_rpm);
-    const float m = P.f_mass, a2 = P.f_a2;
+  // The right-hand side in FP32 at (r - r_plus = d, r, theta, p_r, p_theta).
+  __device__ static void rhs_f(const Params& P, float d, float rf, float thf, float pr, float pth,
+                               const Motion<float>& mo, float f[NV], Trig& tr) {
     float s, c;
     sincosf(thf, &s, &c);
     tr.s = (double)s;
     tr.c = (double)c;
-    const float s2 = s * s;
-    const float sin2th = 2.0f * s * c;
-    const float r2 = rf * rf;
-    const float sig = fmaf(a2, c * c, r2);
-    const float r2a2 = r2 + a2;
-    const float big_a = fmaf(r2a2, r2a2, -a2 * dlt * s2);
-    const float isig = __fdividef(1.0f, sig);
-    const float idlt = __fdividef(1.0f, dlt);
-    const float isd = isig * idlt;
-    const float isd2 = isd * isd;
-    const float isig2 = isig * isig;
-    const float sd = sig * dlt;
-    const float sig_r = 2.0f * rf;
-    const float sig_th = -a2 * sin2th;
-    const float dlt_r = 2.0f * (rf - m);
-    const float a_r = fmaf(4.0f * rf, r2a2, -P.f_two_a2 * (rf - m) * s2);
-    const float a_th = -a2 * dlt * sin2th;
-    const float sd_r = fmaf(sig_r, dlt, sig * dlt_r);
-    const float sd_th = sig_th * dlt;
-    const float g0 = -big_a * isd;
-    const float g1 = P.f_neg_2ma * rf * isd;
-    const float g2 = dlt * isig;
-    const float g3 = isig;
-    const float g5 = fmaf(big_a, sd_r, -a_r * sd) * isd2;
-    const float g6 = P.f_neg_2ma * fmaf(-rf, sd_r, sd) * isd2;
-    const float g7 = fmaf(dlt_r, sig, -dlt * sig_r) * isig2;
-    const float g8 = -sig_r * isig2;
-    const float g10 = fmaf(big_a, sd_th, -a_th * sd) * isd2;
-    const float g11 = P.f_pos_2ma * rf * sd_th * isd2;
-    const float g12 = -dlt * sig_th * isig2;
-    const float g13 = -sig_th * isig2;
-    float g4 = 0.0f, g9 = 0.0f, g14 = 0.0f;
-    if (pph != 0.0f) {  // polar-axis guard
-      const float is2 = __fdividef(1.0f, s2);
-      g4 = fmaf(-a2, s2, dlt) * isd * is2;
-      g9 = fmaf(-sig_r * isig2, is2, a2 * sd_r * isd2);
-      g14 = fmaf(-fmaf(sig_th, s2, sig * sin2th) * isig2, is2 * is2, a2 * sd_th * isd2);
-    }
-    f[CT] = fmaf(g0, pt, g1 * pph);
-    f[CR] = g2 * pr;
-    f[CTH] = g3 * pth;
-    f[CPH] = fmaf(g1, pt, g4 * pph);
-    const float pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
-    f[CPR] = -0.5f * fmaf(g5, pt2, fmaf(2.0f * g6, ptpph, fmaf(g7, pr2, fmaf(g8, pth2, g9 * pph2))));
-    f[CPTH] = -0.5f * fmaf(g10, pt2, fmaf(2.0f * g11, ptpph, fmaf(g12, pr2, fmaf(g13, pth2, g14 * pph2))));
+    rhs_separated<float>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f);
   }
 };
-
 // ------------------------------------------------------------------------------------------
 // The state of one ray between step attempts.
 // ------------------------------------------------------------------------------------------
@@ -444,10 +429,12 @@ __device__ __forceinline__ bool all_finite(const typename M::S y[NV], typename M
 
 // Termination rules in the reference priority (numba_kernel.py:293-311).  Thresholds are
 // compared in the state type like the reference's working-dtype constants.
+// check_finite = false where the state and its right-hand side are already known finite (an
+// accepted step: the attempt checked the candidate and k6; p_t and p_phi never change).
 template <class M>
-__device__ __forceinline__ int classify(const Params& P, const Ray<M>& ry, bool check_h) {
+__device__ __forceinline__ int classify(const Params& P, const Ray<M>& ry, bool check_h, bool check_finite = true) {
   using S = typename M::S;
-  if (!all_finite<M>(ry.y, ry.pt, ry.pph, ry.f)) return FAILURE;
+  if (check_finite && !all_finite<M>(ry.y, ry.pt, ry.pph, ry.f)) return FAILURE;
   if (check_h && ry.h < (S)P.h_min) return FAILURE;
   const S r = ry.y[CR], th = ry.y[CTH];
   if (r < (S)0.0 || th < (S)(-THETA_TOL) || th > (S)(PI + THETA_TOL)) return OUT_OF_DOMAIN;
@@ -476,7 +463,11 @@ __device__ __forceinline__ double carter(const Params& P, const Ray<M>& ry) {
   const double e = -(double)ry.pt;
   const double s = ry.tr.s, c = ry.tr.c;
   double lz2_over_s2 = 0.0;
-  if (lz != 0.0) lz2_over_s2 = (lz * lz) / (s * s);
+  if constexpr (M::kFused) {
+    if (lz != 0.0) lz2_over_s2 = (lz * lz) * rcp_newton<2>(s * s);
+  } else {
+    if (lz != 0.0) lz2_over_s2 = (lz * lz) / (s * s);
+  }
   return p_th * p_th + (c * c) * (lz2_over_s2 - P.a2 * e * e);
 }
 
@@ -496,11 +487,14 @@ __device__ __forceinline__ void ray_init(const Params& P, const double y0[8], do
   // Drift floors (photons/constants.py:163-171): |E0| (1 if E0 == 0), E0^2 M^2.
   double fe = fabs(y0[4]);
   fe = (fe > 0.0) ? fe : 1.0;
+  const double fq = fe * fe * P.mass * P.mass;
+  const double q_den = py_max(fabs(q0), fq);
+  const double e_den = fe * fe;
   ry.ref.q0 = q0;
-  ry.ref.fq = fe * fe * P.mass * P.mass;
-  ry.ref.fe2 = fe * fe;
+  ry.ref.q_den = M::kFused ? 1.0 / q_den : q_den;
+  ry.ref.e_den = M::kFused ? 1.0 / e_den : e_den;
   M::init_rhs(P, ry.y, ry.pt, ry.pph, ry.sh, ry.f, ry.tr);
-  ry.m_null = null_error<M>(ry) / ry.ref.fe2;
+  ry.m_null = drift<M>(null_error<M>(ry), ry.ref.e_den);
   ry.m_q = 0.0;
   ry.lam = 0.0;
   S h = (S)P.h0;
@@ -514,8 +508,7 @@ __device__ __forceinline__ void ray_init(const Params& P, const double y0[8], do
 }
 
 // Step factor min(5, max(0.2, 0.9 en^(-1/5))), 5 for en = 0, capped at 1 after a rejection
-// (numba_kernel.py:272-281).  The fast modes take the power in single precision
-// (en^(-1/5) = 2^(-log2(en)/5)); the reference modes call pow in the working type.
+// (numba_kernel.py:272-281), with pow in the working type (the reference modes).
 template <class M>
 __device__ __forceinline__ typename M::N step_factor(typename M::N en, bool rejected_before) {
   using N = typename M::N;
@@ -524,15 +517,26 @@ __device__ __forceinline__ typename M::N step_factor(typename M::N en, bool reje
     factor = (N)FACTOR_MAX;
   } else {
     N raw;
-    if constexpr (M::kFastFactor) {
-      raw = (N)(0.9f * exp2f(-0.2f * __log2f((float)en)));
-    } else if constexpr (sizeof(N) == 4) {
+    if constexpr (sizeof(N) == 4) {
       // float32 working precision: the power evaluated in double and rounded once to float,
       // i.e. the correctly rounded powf of the reference's float32 ** float32.
       raw = (N)SAFETY * (N)pow((double)en, (double)(N)ERROR_EXPONENT);
     } else {
       raw = (N)SAFETY * pow(en, (N)ERROR_EXPONENT);
     }
+    factor = py_min((N)FACTOR_MAX, py_max((N)FACTOR_MIN, raw));
+  }
+  if (rejected_before) factor = py_min(factor, (N)1.0);
+  return factor;
+}
+
+// The fast modes' step factor from en^2: 0.9 en^(-1/5) = 0.9 (en^2)^(-1/10), in single precision.
+template <class M>
+__device__ __forceinline__ typename M::N step_factor_sq(typename M::N en2, bool rejected_before) {
+  using N = typename M::N;
+  N factor = (N)FACTOR_MAX;
+  if (en2 != (N)0.0) {
+    const N raw = (N)(0.9f * exp2f(-0.1f * __log2f((float)en2)));
     factor = py_min((N)FACTOR_MAX, py_max((N)FACTOR_MIN, raw));
   }
   if (rejected_before) factor = py_min(factor, (N)1.0);
@@ -645,7 +649,9 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   if constexpr (!RK4) {
     if (finite) {
       // HNW scaled RMS norm, pairwise order ((q0+q1)+(q2+q3))+((q4+q5)+(q6+q7)) with the two
-      // constant components contributing exact zeros (numba_kernel.py:261-268).
+      // constant components contributing exact zeros (numba_kernel.py:261-268).  The fast
+      // modes multiply by a Newton reciprocal of the scale and compare en^2 = total / 8 with 1
+      // instead of taking the square root (the step factor is a power of en^2 as well).
       N q[NV];
 #pragma unroll
       for (int i = 0; i < NV; ++i) {
@@ -654,21 +660,38 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
                        c(dp::E6), k6[i]);
         const K e = h * esum;
         const N scale = madd<M>((N)P.atol, (N)P.rtol, py_max((N)fabs(ry.y[i]), (N)fabs(yn[i])));
-        const N v = (N)e / scale;
+        N v;
+        if constexpr (M::kFused) v = (N)e * rcp_newton<1>(scale);
+        else v = (N)e / scale;
         q[i] = v * v;
       }
       // Full-state slots: 0 t, 1 r, 2 th, 3 ph, 4 p_t (0), 5 p_r, 6 p_th, 7 p_phi (0).
       const N total = ((q[CT] + q[CR]) + (q[CTH] + q[CPH])) + (q[CPR] + q[CPTH]);
-      const N en = sqrt(total / (N)8.0);
-      if (!finite_(en)) {
-        finite = false;
-        accept = false;
+      if constexpr (M::kFused) {
+        if (!finite_(total)) {
+          finite = false;
+          accept = false;
+        } else {
+          const N en2 = total * (N)0.125;
+          accept = en2 <= (N)1.0;
+          const N factor = step_factor_sq<M>(en2, ry.rejected_before);
+          if (!(accept && last)) {
+            h_new = (S)((N)h_eff * factor);
+            if ((double)h_new > P.h_max) h_new = (S)P.h_max;
+          }
+        }
       } else {
-        accept = en <= (N)1.0;
-        const N factor = step_factor<M>(en, ry.rejected_before);
-        if (!(accept && last)) {
-          h_new = (S)((N)h_eff * factor);
-          if ((double)h_new > P.h_max) h_new = (S)P.h_max;
+        const N en = sqrt(total / (N)8.0);
+        if (!finite_(en)) {
+          finite = false;
+          accept = false;
+        } else {
+          accept = en <= (N)1.0;
+          const N factor = step_factor<M>(en, ry.rejected_before);
+          if (!(accept && last)) {
+            h_new = (S)((N)h_eff * factor);
+            if ((double)h_new > P.h_max) h_new = (S)P.h_max;
+          }
         }
       }
     }
@@ -703,9 +726,9 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   ry.n_steps += 1;
   ry.h_taken = h_eff;
   // E and L_z drifts are identically zero (p_t, p_phi never change); Q and the null error:
-  ry.m_q = py_max(ry.m_q, fabs(carter<M>(P, ry) - ry.ref.q0) / py_max(fabs(ry.ref.q0), ry.ref.fq));
-  ry.m_null = py_max(ry.m_null, null_error<M>(ry) / ry.ref.fe2);
-  int code = classify<M>(P, ry, true);
+  ry.m_q = py_max(ry.m_q, drift<M>(fabs(carter<M>(P, ry) - ry.ref.q0), ry.ref.q_den));
+  ry.m_null = py_max(ry.m_null, drift<M>(null_error<M>(ry), ry.ref.e_den));
+  int code = classify<M>(P, ry, true, false);
   if (P.disk) {  // disk-plane event, numba_kernel.py:439-454
     const double half_pi = 0.5 * PI;
     const double th_old = (double)y_prev_th;

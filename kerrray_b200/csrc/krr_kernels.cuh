@@ -119,7 +119,15 @@ __global__ void __launch_bounds__(MAXT, MINB)
   bool drained = false;
   long long g = -1;
   int img = 0;
-  unsigned long long my_attempts = 0, my_accepted = 0, my_busy = 0, my_iters = 0;
+  // Lane statistics, added when a photon retires (every busy lane slot is one step attempt).
+  unsigned long long my_attempts = 0, my_accepted = 0;
+  unsigned my_iters = 0;
+  auto retire = [&]() {
+    ray_store<M>(ry, o, g);
+    my_attempts += (unsigned long long)ry.attempts;
+    my_accepted += (unsigned long long)ry.n_steps;
+    atomicAdd(&q->retired, 1ull);
+  };
   while (true) {
     const unsigned idle = __ballot_sync(FULL, !active);
     const int n_idle = __popc(idle);
@@ -138,12 +146,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
           double y0[8];
           photon_source(images, img, Y0, g, y0, q);
           ray_init<M>(im.P, y0, carter_initial(im.P, y0), ry);
-          if (ry.state == RUNNING) {
-            active = true;
-          } else {
-            ray_store<M>(ry, o, g);
-            atomicAdd(&q->retired, 1ull);
-          }
+          if (ry.state == RUNNING) active = true;
+          else retire();
         }
       }
     }
@@ -154,18 +158,13 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     my_iters += 1;
     if (active) {
-      my_busy += 1;
       const Image& im = images[img];
       double* ev = o.event_Y ? o.event_Y + g * 8 : nullptr;
       unsigned char* hit = o.event_hit ? o.event_hit + g : nullptr;
-      const int before = ry.n_steps;
       attempt<M, RK4>(im.P, ry, ev, hit);
-      my_attempts += 1;
-      my_accepted += (unsigned long long)(ry.n_steps - before);
       if (ry.state != RUNNING) {
-        ray_store<M>(ry, o, g);
+        retire();
         active = false;
-        atomicAdd(&q->retired, 1ull);
       }
     }
   }
@@ -174,13 +173,12 @@ __global__ void __launch_bounds__(MAXT, MINB)
   for (int off = 16; off > 0; off >>= 1) {
     my_attempts += __shfl_down_sync(FULL, my_attempts, off);
     my_accepted += __shfl_down_sync(FULL, my_accepted, off);
-    my_busy += __shfl_down_sync(FULL, my_busy, off);
   }
   if (lane == 0) {
     atomicAdd(&q->attempts, my_attempts);
     atomicAdd(&q->accepted, my_accepted);
-    atomicAdd(&q->busy_iters, my_busy);
-    atomicAdd(&q->lane_iters, my_iters * 32ull);
+    atomicAdd(&q->busy_iters, my_attempts);
+    atomicAdd(&q->lane_iters, (unsigned long long)my_iters * 32ull);
   }
 }
 
@@ -254,7 +252,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_bisect_edges(EdgeArgs a) {
   L.ry.state = FAILURE;
   bool active = false, drained = false;
   long long g = -1;
-  unsigned long long my_attempts = 0, my_accepted = 0, my_busy = 0, my_iters = 0;
+  unsigned long long my_attempts = 0, my_accepted = 0;  // every busy lane slot is one attempt
+  unsigned my_iters = 0;
   auto finish_item = [&]() {
     a.lo[g] = L.lo;
     a.hi[g] = L.hi;
@@ -298,12 +297,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_bisect_edges(EdgeArgs a) {
     }
     my_iters += 1;
     if (active) {
-      my_busy += 1;
-      const int before = L.ry.n_steps;
       attempt<M, false>(a.cases[L.c].P, L.ry, nullptr, nullptr);
-      my_attempts += 1;
-      my_accepted += (unsigned long long)(L.ry.n_steps - before);
       if (L.ry.state != RUNNING) {
+        my_attempts += (unsigned long long)L.ry.attempts;
+        my_accepted += (unsigned long long)L.ry.n_steps;
         bool more = edge_next<M>(a, L);
         while (more && L.ry.state != RUNNING) more = edge_next<M>(a, L);
         if (!more) finish_item();
@@ -314,13 +311,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_bisect_edges(EdgeArgs a) {
   for (int off = 16; off > 0; off >>= 1) {
     my_attempts += __shfl_down_sync(FULL, my_attempts, off);
     my_accepted += __shfl_down_sync(FULL, my_accepted, off);
-    my_busy += __shfl_down_sync(FULL, my_busy, off);
   }
   if (lane == 0) {
     atomicAdd(&a.q->attempts, my_attempts);
     atomicAdd(&a.q->accepted, my_accepted);
-    atomicAdd(&a.q->busy_iters, my_busy);
-    atomicAdd(&a.q->lane_iters, my_iters * 32ull);
+    atomicAdd(&a.q->busy_iters, my_attempts);
+    atomicAdd(&a.q->lane_iters, (unsigned long long)my_iters * 32ull);
   }
 }
 

@@ -8,7 +8,7 @@
 // This entry point takes the caller's inputs and outputs and keeps the launch's scratch -- the
 // work-queue counters and the image descriptors -- in a fixed array in this library's device
 // image, so it allocates nothing.  The array is sized for KRR_NOALLOC_MAX_IMAGES images; every
-// GPU that loads the library holds it (the queue plus 128 descriptors of 368 B: about 47 KB) until
+// GPU that loads the library holds it (the queue plus 128 descriptors of 360 B: about 46 KB) until
 // the process exits.
 #include <cuda_runtime.h>
 
