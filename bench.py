@@ -286,41 +286,53 @@ def sweep_edge_errors(K, specs, state: np.ndarray, offsets) -> dict:
 
 
 def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024") -> dict:
-    """Mixed persistent + FP64 re-trace against the plain FP64 kernel on the a*=0.99, i=85 deg
-    image (rtol 1e-6): rays/s of each, whether the two shadow masks are identical, the terminal
-    states' difference and both masks' edge rms against Bardeen's curve."""
+    """Mixed persistent + FP64 settling of the near-critical pixels against the plain FP64 kernel
+    on the a*=0.99, i=85 deg image (rtol 1e-6): rays/s of each pipeline, whether the shadow masks
+    are identical, the terminal states' difference and both masks' edge rms against Bardeen."""
     import torch
 
     specs = workload_specs(K, name)
     total = specs[0].n_rays
     tuned, _ = K.autotune(specs, precision="mixed", device=local)
-    mixed = K.DeviceSweep(specs, precision="mixed", device=local,
-                          launch=K.LaunchConfig(variant=tuned.variant, refill_threshold=tuned.refill_threshold,
-                                                retrace=True))
+
+    def mixed_with(retrace: int):
+        return K.DeviceSweep(specs, precision="mixed", device=local,
+                             launch=K.LaunchConfig(variant=tuned.variant, refill_threshold=tuned.refill_threshold,
+                                                   retrace=retrace))
+
+    crit, edge, bare = mixed_with(K.RETRACE_CRITICAL), mixed_with(K.RETRACE_EDGE), mixed_with(0)
     fast = K.DeviceSweep(specs, precision="fast64", device=local, launch=K.autotune(specs, precision="fast64", device=local)[0])
     plain = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True))
-    for sw in (mixed, fast, plain):
+    sweeps = (crit, edge, bare, fast, plain)
+    for sw in sweeps:
         sw.run()
-    t_mixed = min(_timed_steps(mixed, 3, stream, flush))
-    t_fast = min(_timed_steps(fast, 3, stream, flush))
-    t_plain = min(_timed_steps(plain, 2, stream, flush))
-    ms = mixed.stats()
-    same = bool(torch.equal(mixed.tensors["state"], plain.tensors["state"]))
-    differ = int((mixed.tensors["state"] != plain.tensors["state"]).sum().item())
-    esc = (plain.tensors["state"] == 1) & (mixed.tensors["state"] == 1)
-    rel = ((mixed.tensors["Y"] - plain.tensors["Y"]).abs() / plain.tensors["Y"].abs().clamp_min(1.0)).amax(dim=1)
-    st_plain = plain.tensors["state"].cpu().numpy()
-    st_mixed = mixed.tensors["state"].cpu().numpy()
+    t = {k: min(_timed_steps(sw, 3 if k != "plain" else 2, stream, flush))
+         for k, sw in zip(("crit", "edge", "bare", "fast", "plain"), sweeps)}
+    cs, es = crit.stats(), edge.stats()
+    ref = plain.tensors["state"]
+    esc = (ref == 1) & (crit.tensors["state"] == 1)
+    rel = ((crit.tensors["Y"] - plain.tensors["Y"]).abs() / plain.tensors["Y"].abs().clamp_min(1.0)).amax(dim=1)
+    st_plain = ref.cpu().numpy()
+    st_mixed = crit.tensors["state"].cpu().numpy()
     out = {"workload": WORKLOADS[name], "photons": total,
-           "mixed_retrace_rays_s": total / (t_mixed * 1e-3), "fast64_rays_s": total / (t_fast * 1e-3),
-           "plain_fp64_rays_s": total / (t_plain * 1e-3), "speedup_mixed_vs_plain": t_plain / t_mixed,
-           "mask_identical": same, "pixels_differing": differ, "retraced": int(ms["retraced"]),
+           "mixed_pipeline_rays_s": total / (t["crit"] * 1e-3), "plain_fp64_rays_s": total / (t["plain"] * 1e-3),
+           "speedup_mixed_vs_plain": t["plain"] / t["crit"],
+           "mask_identical": bool(torch.equal(crit.tensors["state"], ref)),
+           "pixels_differing": int((crit.tensors["state"] != ref).sum().item()),
+           "critical": int(cs["critical"]), "rechecked": int(cs["rechecked"]),
+           "pipeline": "analytic critical set in reference-order FP64 beside the mixed trace, then a re-trace of "
+                       "every photon unlike its analytic class",
+           "mixed_kernel_only_rays_s": total / (t["bare"] * 1e-3),
+           "mixed_edge_retrace_rays_s": total / (t["edge"] * 1e-3),
+           "edge_retrace_mask_identical": bool(torch.equal(edge.tensors["state"], ref)),
+           "edge_retraced": int(es["retraced"]),
+           "fast64_rays_s": total / (t["fast"] * 1e-3),
            "escaped_max_rel_dY_vs_plain": float(rel[esc].max().item()),
            "escaped_median_rel_dY_vs_plain": float(rel[esc].median().item()),
            "edge_rms_px_plain": edge_rms_px(K, specs[0], st_plain),
            "edge_rms_px_mixed": edge_rms_px(K, specs[0], st_mixed),
            "mixed_launch": {"variant": tuned.variant, "refill_threshold": tuned.refill_threshold}}
-    for sw in (mixed, fast, plain):
+    for sw in sweeps:
         sw.close()
     return out
 

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define KRR_ABI_VERSION 1
+#define KRR_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define KRR_API __attribute__((visibility("default")))
@@ -55,6 +55,19 @@ enum {
   KRR_PREC_REFERENCE = 0, /* reference operation order, no contraction; FP64 or the FP32 dtype */
   KRR_PREC_FAST64 = 1,    /* FP64 with FMA contraction, sincos and reciprocals                */
   KRR_PREC_MIXED = 2      /* FP32 stages, FP64 state accumulation, Delta and error norm       */
+};
+
+/* FP64 re-trace after (or beside) a mixed-precision trace (krr_launch.retrace). */
+enum {
+  KRR_RETRACE_NONE = 0,
+  KRR_RETRACE_EDGE = 1,     /* after the trace: every pixel that did not end ESCAPED or CAPTURED or
+                               whose code differs from one of its 8 neighbours */
+  KRR_RETRACE_CRITICAL = 2  /* before the trace, each photon's analytic class from its constants of
+                               motion (radial potential R(r)); photons within a band of the
+                               critical curve run in reference order on SMs of their own, beside
+                               the main trace; afterwards photons whose code is not their analytic
+                               class are traced again in FP64, and what still disagrees (or ended
+                               within 1 % of its affine or step budget) in reference order */
 };
 
 /* termination codes (photons/classification.py:60-69) */
@@ -120,10 +133,9 @@ typedef struct krr_launch {
   int32_t refill_threshold;  /* idle lanes of a warp before it refills from the queue */
   int32_t plain;             /* 1: one thread per photon, no work queue (the plain kernel) */
   int32_t variant;           /* compiled launch shape of the persistent kernel (krr_list_variants) */
-  int32_t retrace;           /* 1: after the trace, flag every pixel that did not end ESCAPED or
-                                CAPTURED or whose code differs from one of its 8 neighbours, and
-                                trace those again with the reference-order FP64 kernel (rk45,
-                                float64, persistent launches) */
+  int32_t retrace;           /* KRR_RETRACE_*: settle the pixels a mixed trace could classify
+                                differently with the reference-order FP64 kernel (rk45, float64,
+                                persistent launches) */
   int32_t reserved;
 } krr_launch;
 
@@ -143,9 +155,12 @@ typedef struct krr_stats {
   uint64_t lane_slots;  /* warp iterations x 32 */
   uint64_t busy_slots;  /* lane slots that advanced a running photon */
   double kernel_ms;     /* device time of the trace kernel (CUDA events on its stream) */
-  uint64_t retraced;    /* photons traced again in FP64 (retrace on) */
+  uint64_t retraced;    /* photons traced in reference-order FP64 by the re-trace */
   uint64_t retrace_attempts;
-  double retrace_ms;    /* device time of the flagging and the re-trace */
+  double retrace_ms;    /* device time of the flagging and the re-trace after the main trace */
+  uint64_t critical;    /* KRR_RETRACE_CRITICAL: photons in the critical band (traced beside) */
+  uint64_t rechecked;   /* KRR_RETRACE_CRITICAL: photons traced again after the check */
+  double critical_ms;   /* KRR_RETRACE_CRITICAL: device time of the critical-set kernel */
 } krr_stats;
 
 KRR_API const char* krr_last_error(void);
@@ -183,6 +198,14 @@ KRR_API int krr_trace_images(int device, const krr_image* images, int32_t n_imag
  * by the caller; stream as above.  Synchronises the stream before returning (the statistics
  * are read back). */
 KRR_API size_t krr_workspace_size(int32_t n_images, int64_t retrace_photons);
+
+/* Analytic class of n initial states (host arrays; no device needed): 0 escapes, 1 is captured,
+ * 2 lies within the critical band (risk_band: max(2e-3, 2e3 rtol) M in the image plane) of the
+ * boundary between the two, or is not an inward ray outside r_+ + horizon_epsilon.  From the
+ * radial potential of the photon's constants of motion (Carter 1968); the classes the
+ * KRR_RETRACE_CRITICAL pipeline uses.  No counterpart in the reference. */
+KRR_API int krr_analytic_classes(double mass, double spin, double rtol, double horizon_epsilon, const double* Y0,
+                                 int64_t n, uint8_t* out);
 
 /* The launch shapes compiled for (precision, options.method, options.dtype): *count receives
  * their number; up to max_out are described in out (nullable) for `device`.  Measurement

@@ -37,7 +37,17 @@ from kerrray_b200.camera import Camera, initial_states, initial_states_at
 from kerrray_b200.orbits import critical_impact_parameters, shadow_curve
 from kerrray_b200.rays import concatenate_results, trace_rays
 from kerrray_b200.shadow import FAILURE_STATES, ShadowImage, compute_shadow, shadow_mask_int8, state_counts
-from kerrray_b200.sweep import DeviceSweep, ImageSpec, LaunchConfig, SweepResult, order_by_cost, trace_images
+from kerrray_b200.sweep import (
+    RETRACE_CRITICAL,
+    RETRACE_EDGE,
+    DeviceSweep,
+    ImageSpec,
+    LaunchConfig,
+    SweepResult,
+    analytic_classes,
+    order_by_cost,
+    trace_images,
+)
 from kerrray_b200.validation import (
     critical_impacts,
     equatorial_photon,
@@ -70,4 +80,5 @@ __all__ = [
     "SweepResult", "TerminationOptions", "TerminationState", "autotune", "available_backends", "compute_shadow",
     "concatenate_results", "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
     "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
+    "RETRACE_CRITICAL", "RETRACE_EDGE", "analytic_classes",
 ]

@@ -27,7 +27,7 @@ EXPORTS = (
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
     "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
     "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy", "krr_bisect_edges",
-    "krr_lensing_workspace_size", "krr_lensing_adjoint", "krr_lensing_replay",
+    "krr_lensing_workspace_size", "krr_lensing_adjoint", "krr_lensing_replay", "krr_analytic_classes",
 )
 
 
@@ -83,7 +83,8 @@ class KrrStats(ctypes.Structure):
     _fields_ = [("photons", ctypes.c_uint64), ("retired", ctypes.c_uint64), ("attempts", ctypes.c_uint64),
                 ("accepted", ctypes.c_uint64), ("lane_slots", ctypes.c_uint64), ("busy_slots", ctypes.c_uint64),
                 ("kernel_ms", ctypes.c_double), ("retraced", ctypes.c_uint64), ("retrace_attempts", ctypes.c_uint64),
-                ("retrace_ms", ctypes.c_double)]
+                ("retrace_ms", ctypes.c_double), ("critical", ctypes.c_uint64), ("rechecked", ctypes.c_uint64),
+                ("critical_ms", ctypes.c_double)]
 
     def as_dict(self) -> dict[str, Any]:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -127,6 +128,8 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(KrrResult), ctypes.POINTER(KrrStats)]
         L.krr_workspace_size.restype = ctypes.c_size_t
         L.krr_workspace_size.argtypes = [i32, i64]
+        L.krr_analytic_classes.restype = ctypes.c_int
+        L.krr_analytic_classes.argtypes = [dp, dp, dp, dp, vp, i64, vp]
         L.krr_trace_images_device.restype = ctypes.c_int
         L.krr_trace_images_device.argtypes = [ctypes.c_int, ctypes.POINTER(KrrImage), i32, vp,
                                               ctypes.POINTER(KrrLaunch), ctypes.POINTER(KrrResult), vp,

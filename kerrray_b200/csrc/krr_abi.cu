@@ -365,28 +365,40 @@ int persistent_shape(int device, int32_t precision, const krr_options* o, const 
   return KRR_OK;
 }
 
-// Device layout of a batched launch's workspace: the main and the re-trace queue counters, the
-// image descriptors, then the re-trace list (one int64 per photon when the re-trace is on).
+// Device layout of a batched launch's workspace: four queue counters (the main trace; the
+// reference-order trace of the edge or of the critical photons; with the critical set, the
+// FP64 re-trace of photons unlike their analytic class and the reference-order re-trace of
+// what remains), the image descriptors, then, with the re-trace on, the photon list (one
+// int64 per photon) and the analytic classes (one byte per photon).
 struct WorkLayout {
   krr::Queue* q0;
   krr::Queue* q1;
+  krr::Queue* q2;
+  krr::Queue* q3;
   krr::Image* images;
   long long* list;
+  unsigned char* risk;
 };
 
 constexpr size_t round256(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t kQueueArea = 1024;
 
 size_t work_bytes(int n_images, long long list_entries) {
-  return 512 + round256((size_t)std::max(n_images, 0) * sizeof(krr::Image)) + (size_t)std::max(list_entries, 0LL) * 8;
+  const size_t n = (size_t)std::max(list_entries, 0LL);
+  return kQueueArea + round256((size_t)std::max(n_images, 0) * sizeof(krr::Image)) + round256(n * 8) + n;
 }
 
-WorkLayout work_layout(void* base, int n_images) {
+WorkLayout work_layout(void* base, int n_images, long long list_entries) {
   char* b = static_cast<char*>(base);
   WorkLayout w;
   w.q0 = reinterpret_cast<krr::Queue*>(b);
   w.q1 = reinterpret_cast<krr::Queue*>(b + 256);
-  w.images = reinterpret_cast<krr::Image*>(b + 512);
-  w.list = reinterpret_cast<long long*>(b + 512 + round256((size_t)n_images * sizeof(krr::Image)));
+  w.q2 = reinterpret_cast<krr::Queue*>(b + 512);
+  w.q3 = reinterpret_cast<krr::Queue*>(b + 768);
+  const size_t list_at = kQueueArea + round256((size_t)n_images * sizeof(krr::Image));
+  w.images = reinterpret_cast<krr::Image*>(b + kQueueArea);
+  w.list = reinterpret_cast<long long*>(b + list_at);
+  w.risk = reinterpret_cast<unsigned char*>(b + list_at + round256((size_t)std::max(list_entries, 0LL) * 8));
   return w;
 }
 
@@ -400,13 +412,24 @@ struct Pipeline {
   int32_t precision = KRR_PREC_FAST64;
   bool dtype32 = false, rk4 = false, disk = false;
   bool retrace = false;
+  int retrace_mode = 0;  // KRR_RETRACE_*
   WorkLayout w{};
   krr_result out{};
   krr::PersistArgs main{};
   const krr::Variant* main_v = nullptr;
   krr::PersistArgs re{};
   const krr::Variant* re_v = nullptr;
+  krr::PersistArgs crit{};  // KRR_RETRACE_CRITICAL: the critical photons, on SMs of their own
+  const krr::Variant* crit_v = nullptr;
+  krr::PersistArgs fix{};   // the FP64 re-trace of photons unlike their analytic class
+  const krr::Variant* fix_v = nullptr;
 };
+
+// Registers one resident block of a kernel holds (allocated per warp in units of 256).
+int block_registers(int threads, int regs_per_thread) {
+  const int warps = (threads + 31) / 32;
+  return warps * ((regs_per_thread * 32 + 255) / 256 * 256);
+}
 
 int prepare_pipeline(int device, const krr_image* images, int n_images, long long total, const double* d_Y0,
                      const krr_launch* launch, const krr_result* d_out, void* d_work, size_t work_size, Pipeline& p) {
@@ -423,12 +446,20 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
   p.disk = o0->disk_plane != 0;
   p.plain = launch && launch->plain;
   p.plain_block = (launch && launch->block > 0 && launch->block % 32 == 0) ? launch->block : 128;
-  p.retrace = launch && launch->retrace;
+  p.retrace_mode = launch ? launch->retrace : 0;
+  if (p.retrace_mode < KRR_RETRACE_NONE || p.retrace_mode > KRR_RETRACE_CRITICAL)
+    return fail(KRR_ERR_INVALID, "retrace must be 0, 1 (edge) or 2 (critical), got %d", p.retrace_mode);
+  p.retrace = p.retrace_mode != KRR_RETRACE_NONE;
   if (p.retrace && (p.rk4 || p.dtype32 || p.plain))
     return fail(KRR_ERR_UNSUPPORTED, "the FP64 re-trace follows persistent rk45 float64 launches only");
+  if (p.retrace_mode == KRR_RETRACE_CRITICAL) {
+    for (int k = 0; k < n_images; ++k)
+      if (images[k].options.disk_plane)
+        return fail(KRR_ERR_UNSUPPORTED, "the critical-set re-trace classifies ESCAPED/CAPTURED only (no disk events)");
+  }
   const size_t need = work_bytes(n_images, p.retrace ? total : 0);
   if (work_size < need) return fail(KRR_ERR_INVALID, "workspace of %zu bytes is smaller than the %zu needed", work_size, need);
-  p.w = work_layout(d_work, n_images);
+  p.w = work_layout(d_work, n_images, p.retrace ? total : 0);
   p.out = *d_out;
   LaunchShape shape{};
   rc = persistent_shape(device, precision, o0, launch, shape);
@@ -458,14 +489,76 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     p.re.index = p.w.list;
     p.re.d_total = &p.w.q0->flagged;
   }
+  if (p.retrace_mode == KRR_RETRACE_CRITICAL) {
+    // The reference-order kernel takes the critical photons on 1/18 of the SMs: launched first,
+    // each of its blocks fills an SM's register file, and it lets the main (mixed) trace launch
+    // as soon as its blocks run (programmatic dependent launch), so the main trace -- which
+    // skips the critical photons -- spreads over the other SMs and the two run side by side.
+    // The main trace waits for it only at its exit.  Afterwards the photons unlike their
+    // analytic class are traced again in fast FP64, and what still disagrees (or ended near
+    // its budget) in reference order.
+    const krr::Variant* wv = krr::ref_wide_variant();
+    if (wv->occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "the critical-set kernel cannot be resident");
+    const int sms = std::max(sm_count_of(device), 2);
+    const int crit_sms = std::max(1, sms / 18);
+    const int bps = std::max(1, p.main.grid / sms);
+    p.main.grid = (sms - crit_sms) * bps;
+    p.main.risk = p.w.risk;
+    p.main.pdl = krr::PDL_WAIT;
+    p.crit = p.main;
+    p.crit_v = wv;
+    p.crit.q = p.w.q1;
+    p.crit.grid = crit_sms;
+    p.crit.block = wv->block;
+    p.crit.refill_threshold = 1;
+    p.crit.index = p.w.list;
+    p.crit.d_total = &p.w.q1->flagged;
+    p.crit.risk = nullptr;
+    p.crit.spread = 1;
+    p.crit.pdl = krr::PDL_TRIGGER | krr::PDL_STAMP;
+    int nf = 0;
+    const krr::Variant* fv = krr::fast_variants(false, false, &nf);
+    if (!fv || nf < 1 || fv[0].occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "no FP64 re-trace kernel");
+    p.fix_v = &fv[0];
+    p.fix = p.crit;
+    p.fix.q = p.w.q2;
+    p.fix.grid = sms * fv[0].occupancy();
+    p.fix.block = fv[0].block;
+    p.fix.d_total = &p.w.q2->flagged;
+    p.fix.pdl = 0;
+    p.re = p.fix;
+    p.re.q = p.w.q3;
+    p.re.grid = sms * p.re_v->occupancy();
+    p.re.block = p.re_v->block;
+    p.re.d_total = &p.w.q3->flagged;
+  }
   return KRR_OK;
 }
 
 // The launch sequence (also what a plan captures): clear the counters, trace, and, with the
 // re-trace on, flag the edge and failed pixels and trace them again in reference-order FP64.
 // Events (nullable) bracket the main kernel (ev0, ev1) and the re-trace (ev1, ev2).
+cudaError_t enqueue_critical(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t ev2) {
+  cudaError_t e = cudaMemsetAsync(p.w.q0, 0, kQueueArea, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&p.w.q1->t_first, 0xff, sizeof(unsigned long long), s);
+  if (e == cudaSuccess && ev0) e = cudaEventRecord(ev0, s);
+  const long long* state = reinterpret_cast<const long long*>(p.out.state);
+  if (e == cudaSuccess)
+    e = krr::risk_prepass(p.w.images, p.n_images, p.total, p.main.Y0, p.w.risk, p.w.list, p.w.q1, s);
+  if (e == cudaSuccess) e = p.crit_v->run(p.crit, s);  // critical photons, reference order
+  if (e == cudaSuccess) e = p.main_v->run(p.main, s);  // programmatic dependent: runs beside it
+  if (e == cudaSuccess && ev1) e = cudaEventRecord(ev1, s);
+  if (e == cudaSuccess) e = krr::check_risk(p.w.images, p.n_images, p.total, p.w.risk, state, p.w.list, p.w.q2, false, s);
+  if (e == cudaSuccess) e = p.fix_v->run(p.fix, s);
+  if (e == cudaSuccess) e = krr::check_risk(p.w.images, p.n_images, p.total, p.w.risk, state, p.w.list, p.w.q3, true, s);
+  if (e == cudaSuccess) e = p.re_v->run(p.re, s);
+  if (e == cudaSuccess && ev2) e = cudaEventRecord(ev2, s);
+  return e;
+}
+
 cudaError_t enqueue_pipeline(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, cudaEvent_t ev2) {
-  cudaError_t e = cudaMemsetAsync(p.w.q0, 0, 512, s);
+  if (p.retrace_mode == KRR_RETRACE_CRITICAL) return enqueue_critical(p, s, ev0, ev1, ev2);
+  cudaError_t e = cudaMemsetAsync(p.w.q0, 0, kQueueArea, s);
   if (e == cudaSuccess && p.out.event_Y) e = cudaMemsetAsync(p.out.event_Y, 0, (size_t)p.total * 8 * sizeof(double), s);
   if (e == cudaSuccess && p.out.event_hit) e = cudaMemsetAsync(p.out.event_hit, 0, (size_t)p.total, s);
   if (e == cudaSuccess && ev0) e = cudaEventRecord(ev0, s);
@@ -496,14 +589,18 @@ cudaError_t enqueue_pipeline(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0,
 // Read the counters back (synchronises the stream) and check the queue's bookkeeping.
 int finish_pipeline(const Pipeline& p, cudaStream_t s, krr_stats* stats, cudaEvent_t ev0, cudaEvent_t ev1,
                     cudaEvent_t ev2) {
-  krr::Queue q[2];
+  krr::Queue q[4];
   std::memset(q, 0, sizeof(q));
   KRR_CUDA(cudaMemcpyAsync(&q[0], p.w.q0, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaMemcpyAsync(&q[1], p.w.q1, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaMemcpyAsync(&q[2], p.w.q2, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaMemcpyAsync(&q[3], p.w.q3, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaStreamSynchronize(s));
+  const bool crit = p.retrace_mode == KRR_RETRACE_CRITICAL;
   float ms = 0.0f, ms2 = 0.0f;
   if (ev0 && ev1) KRR_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   if (ev1 && ev2) KRR_CUDA(cudaEventElapsedTime(&ms2, ev1, ev2));
+  const double ms_c = (crit && q[1].t_last >= q[1].t_first) ? 1e-6 * (double)(q[1].t_last - q[1].t_first) : 0.0;
   if (stats) {
     stats->photons = (uint64_t)p.total;
     stats->retired = q[0].retired;
@@ -512,15 +609,22 @@ int finish_pipeline(const Pipeline& p, cudaStream_t s, krr_stats* stats, cudaEve
     stats->lane_slots = q[0].lane_iters;
     stats->busy_slots = q[0].busy_iters;
     stats->kernel_ms = ms;
-    stats->retraced = p.retrace ? q[0].flagged : 0;
-    stats->retrace_attempts = q[1].attempts;
+    stats->retraced = crit ? q[1].flagged + q[2].flagged + q[3].flagged : (p.retrace ? q[0].flagged : 0);
+    stats->retrace_attempts = q[1].attempts + q[2].attempts + q[3].attempts;
     stats->retrace_ms = p.retrace ? ms2 : 0.0;
+    stats->critical = crit ? q[1].flagged : 0;
+    stats->critical_ms = ms_c;
+    stats->rechecked = crit ? q[2].flagged + q[3].flagged : 0;
   }
-  if (q[0].error || q[1].error)
+  if (q[0].error || q[1].error || q[2].error || q[3].error)
     return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
   if (q[0].retired != (unsigned long long)p.total)
     return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu photons retired of %lld", q[0].retired, p.total);
-  if (p.retrace && q[1].retired != q[0].flagged)
+  if (crit && (q[1].retired != q[1].flagged || q[2].retired != q[2].flagged || q[3].retired != q[3].flagged))
+    return fail(KRR_ERR_CUDA, "critical-set inconsistency: %llu of %llu critical, %llu of %llu and %llu of %llu "
+                "rechecked photons retired", q[1].retired, q[1].flagged, q[2].retired, q[2].flagged, q[3].retired,
+                q[3].flagged);
+  if (p.retrace && !crit && q[1].retired != q[0].flagged)
     return fail(KRR_ERR_CUDA, "re-trace inconsistency: %llu photons retired of %llu flagged", q[1].retired, q[0].flagged);
   return KRR_OK;
 }
@@ -710,6 +814,19 @@ int krr_list_variants(int device, int32_t precision, const krr_options* options,
 }
 
 size_t krr_workspace_size(int32_t n_images, int64_t retrace_photons) { return work_bytes(n_images, retrace_photons); }
+
+int krr_analytic_classes(double mass, double spin, double rtol, double horizon_epsilon, const double* Y0, int64_t n,
+                         uint8_t* out) {
+  int rc = validate_spacetime(mass, spin);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!Y0 || !out))) return fail(KRR_ERR_INVALID, "Y0 and out must hold n >= 0 rows");
+  if (!(rtol > 0.0) || !(horizon_epsilon >= 0.0)) return fail(KRR_ERR_INVALID, "rtol must be > 0 and horizon_epsilon >= 0");
+  const double a = spin * mass;
+  const double r_capture = outer_horizon(mass, a) + horizon_epsilon;
+  const double band = krr::risk_band(mass, rtol);
+  for (int64_t i = 0; i < n; ++i) out[i] = (uint8_t)krr::radial_risk(mass, a, r_capture, Y0 + 8 * i, band);
+  return KRR_OK;
+}
 
 int krr_trace_images_device(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
                             const krr_launch* launch, const krr_result* d_out, void* workspace, size_t workspace_bytes,

@@ -124,14 +124,15 @@ __device__ __forceinline__ double surface_radius(const Params& P, int state) {
 // recorded stage sums for the reverse pass.
 __device__ __forceinline__ void fixed_step(const Params& P, Ray<Fast64>& ry, double h, double acc[6][NV],
                                            double k[6][NV]) {
-  double yn[NV];
+  double yn[NV], esum[NV];
   Trig tr;
-  dp_stages<Fast64, false>(P, ry, h, k[0], k[1], k[2], k[3], k[4], k[5], yn, tr, acc);
+  dp_stages<Fast64, false>(P, ry, h, k[5], yn, esum, tr, acc);
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
     ry.y[i] = yn[i];
     ry.f[i] = k[5][i];
   }
+  ry.tr = tr;  // sin and cos at the new state: the next step's stages shift from them
 }
 
 // Replaces the last accepted step (y_prev -> ry, length h_last) by the DP5 step from y_prev

@@ -82,8 +82,10 @@ struct Params {
 // of the integration here, so only Q0 and the two denominators of the drifts are kept:
 // max(|Q0|, E0^2 M^2) for the Carter constant and E0^2 for the null error.  The reference
 // modes divide by them; the fast modes keep their reciprocals and multiply.
+template <class D>
 struct Refs {
-  double q0, q_den, e_den;
+  double q0;
+  D q_den, e_den;
 };
 
 // x / den in the reference modes, x * den (den holding the reciprocal) in the fast modes.
@@ -135,9 +137,10 @@ struct Trig {
 // always FP64 and cast to W before it meets the momenta.
 template <class W>
 struct RefMode {
-  using S = W;  // state type
-  using K = W;  // stage type
-  using N = W;  // error-norm type
+  using S = W;       // state type
+  using K = W;       // stage type
+  using N = W;       // error-norm type
+  using D = double;  // diagnostics (running maxima and their denominators)
   static constexpr bool kFused = false;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
@@ -147,7 +150,7 @@ struct RefMode {
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow&, K f[NV], Trig& tr) {
     rhs(P, y[CR], y[CTH], pt, y[CPR], y[CPTH], pph, f, tr);
   }
-  __device__ static void accepted(const Params&, const S[NV], Shadow&) {}
+  __device__ static void accepted(const Params&, const S[NV], Shadow&, const Trig&) {}
 
   // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state).
   template <bool LAST, class R>
@@ -255,6 +258,32 @@ __device__ __forceinline__ double rcp_newton(double x) {
 __device__ __forceinline__ double rcp_fast(double x) { return rcp_newton<2>(x); }
 __device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
 
+// sin and cos of theta0 + d from s0 = sin(theta0), c0 = cos(theta0) by the angle-addition
+// formulas, with sin d and cos d from their Taylor series: through d^7 and d^6 in FP32
+// (|d| <= 1/4: truncation below 4e-10), through d^9 and d^10 in FP64 (|d| <= 1/10: below
+// 3e-19).  The stages of one step move theta by such small amounts, so this replaces a full
+// sincos (argument reduction and two polynomials) by about a dozen fused operations.
+// Returns false, computing nothing, when |d| exceeds the range.
+__device__ __forceinline__ bool sincos_shift(float s0, float c0, float d, float& s, float& c) {
+  if (!(fabsf(d) <= 0.25f)) return false;
+  const float d2 = d * d;
+  const float sd = d * fmaf(d2, fmaf(d2, fmaf(d2, -1.0f / 5040.0f, 1.0f / 120.0f), -1.0f / 6.0f), 1.0f);
+  const float cd = fmaf(d2, fmaf(d2, fmaf(d2, -1.0f / 720.0f, 1.0f / 24.0f), -0.5f), 1.0f);
+  s = fmaf(s0, cd, c0 * sd);
+  c = fmaf(c0, cd, -(s0 * sd));
+  return true;
+}
+__device__ __forceinline__ bool sincos_shift(double s0, double c0, double d, double& s, double& c) {
+  if (!(fabs(d) <= 0.1)) return false;
+  const double d2 = d * d;
+  const double sd = d * fma(d2, fma(d2, fma(d2, fma(d2, 1.0 / 362880.0, -1.0 / 5040.0), 1.0 / 120.0), -1.0 / 6.0), 1.0);
+  const double cd =
+      fma(d2, fma(d2, fma(d2, fma(d2, fma(d2, -1.0 / 3628800.0, 1.0 / 40320.0), -1.0 / 720.0), 1.0 / 24.0), -0.5), 1.0);
+  s = fma(s0, cd, c0 * sd);
+  c = fma(c0, cd, -(s0 * sd));
+  return true;
+}
+
 // Per-ray constants of the separated form.
 template <class T>
 struct Motion {
@@ -300,6 +329,7 @@ struct Fast64 {
   using S = double;
   using K = double;
   using N = double;
+  using D = float;  // the drift maxima: FP64 values, kept to single precision
   static constexpr bool kFused = true;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
@@ -309,19 +339,28 @@ struct Fast64 {
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow&, K f[NV], Trig& tr) {
     rhs(P, y[CR], y[CTH], pt, y[CPR], y[CPTH], pph, f, tr);
   }
-  __device__ static void accepted(const Params&, const S[NV], Shadow&) {}
+  __device__ static void accepted(const Params&, const S[NV], Shadow&, const Trig&) {}
 
   // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state).
+  // Stages 1..5 take sin and cos of their theta from the accepted state's (ry.tr, exact) by a
+  // small-angle shift; the last stage evaluates them exactly at the candidate, whose trig then
+  // serves the classification, the diagnostics and the next step.
   template <bool LAST, class R>
   __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
     S ys[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) ys[i] = upd<Fast64>(ry.y[i], h, acc[i]);
+    double s, c;
     if constexpr (LAST) {
 #pragma unroll
       for (int i = 0; i < NV; ++i) yn[i] = ys[i];
+      sincos(ys[CTH], &s, &c);
+    } else {
+      if (!sincos_shift(ry.tr.s, ry.tr.c, ys[CTH] - ry.y[CTH], s, c)) sincos(ys[CTH], &s, &c);
     }
-    rhs(P, ys[CR], ys[CTH], ry.pt, ys[CPR], ys[CPTH], ry.pph, f, tr);
+    tr.s = s;
+    tr.c = c;
+    rhs_sc(P, ys[CR], s, c, ry.pt, ys[CPR], ys[CPTH], ry.pph, f);
   }
 
   __device__ static void rhs(const Params& P, double r, double th, double pt, double pr, double pth, double pph,
@@ -330,6 +369,11 @@ struct Fast64 {
     sincos(th, &s, &c);
     tr.s = s;
     tr.c = c;
+    rhs_sc(P, r, s, c, pt, pr, pth, pph, f);
+  }
+
+  __device__ static void rhs_sc(const Params& P, double r, double s, double c, double pt, double pr, double pth,
+                                double pph, double f[NV]) {
     Motion<double> mo;
     mo.set(pt, pph, P.a);
     rhs_separated<double>(fma(r, r - P.two_m, P.a2), r, s, c, pr, pth, mo, P.a, P.a2, P.mass, f);
@@ -344,12 +388,13 @@ struct Mixed {
   using S = double;
   using K = float;
   using N = double;
+  using D = float;
   static constexpr bool kFused = true;
 
-  // FP32 copy of what the stages read: r - r_plus, r, theta, p_r, p_theta, and the ray's
-  // constants of motion.
+  // FP32 copy of what the stages read: r - r_plus, r, theta with its sine and cosine, p_r,
+  // p_theta, and the ray's constants of motion.
   struct Shadow {
-    float d0, r, th, pr, pth;
+    float d0, r, th, s0, c0, pr, pth;
     Motion<float> mo;
   };
 
@@ -360,38 +405,43 @@ struct Mixed {
     return t;
   }
 
-  __device__ static void accepted(const Params& P, const S y[NV], Shadow& sh) {
+  // tr: the accepted state's FP64 sine and cosine (accept_trig).
+  __device__ static void accepted(const Params& P, const S y[NV], Shadow& sh, const Trig& tr) {
     sh.d0 = (float)(y[CR] - P.r_plus);
     sh.r = (float)y[CR];
     sh.th = (float)y[CTH];
+    sh.s0 = (float)tr.s;
+    sh.c0 = (float)tr.c;
     sh.pr = (float)y[CPR];
     sh.pth = (float)y[CPTH];
   }
 
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow& sh, K f[NV], Trig& tr) {
     sh.mo.set((float)pt, (float)pph, (float)P.a);
-    accepted(P, y, sh);
-    rhs_f(P, sh.d0, sh.r, sh.th, sh.pr, sh.pth, sh.mo, f, tr);
+    tr = accept_trig(y[CTH], tr);
+    accepted(P, y, sh, tr);
+    rhs_f(P, sh.d0, sh.r, sh.s0, sh.c0, sh.pr, sh.pth, sh.mo, f);
   }
 
+  // Every stage's sine and cosine come from the accepted state's by a small-angle shift; near
+  // the axis (|sin| < 1/50, where the shift's sum would cancel) or for a large shift, sincosf.
   template <bool LAST, class R>
-  __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
+  __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig&, S yn[NV]) {
+    const Shadow& sh = ry.sh;
+    const float dth = h * acc[CTH];
+    float s, c;
+    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift(sh.s0, sh.c0, dth, s, c))) sincosf(sh.th + dth, &s, &c);
+    rhs_f(P, fmaf(h, acc[CR], sh.d0), fmaf(h, acc[CR], sh.r), s, c, fmaf(h, acc[CPR], sh.pr), fmaf(h, acc[CPTH], sh.pth),
+          sh.mo, f);
     if constexpr (LAST) {
 #pragma unroll
       for (int i = 0; i < NV; ++i) yn[i] = ry.y[i] + (double)(h * acc[i]);  // FP64 accumulation
     }
-    const Shadow& sh = ry.sh;
-    rhs_f(P, fmaf(h, acc[CR], sh.d0), fmaf(h, acc[CR], sh.r), fmaf(h, acc[CTH], sh.th), fmaf(h, acc[CPR], sh.pr),
-          fmaf(h, acc[CPTH], sh.pth), sh.mo, f, tr);
   }
 
-  // The right-hand side in FP32 at (r - r_plus = d, r, theta, p_r, p_theta).
-  __device__ static void rhs_f(const Params& P, float d, float rf, float thf, float pr, float pth,
-                               const Motion<float>& mo, float f[NV], Trig& tr) {
-    float s, c;
-    sincosf(thf, &s, &c);
-    tr.s = (double)s;
-    tr.c = (double)c;
+  // The right-hand side in FP32 at (r - r_plus = d, r, sin, cos, p_r, p_theta).
+  __device__ static void rhs_f(const Params& P, float d, float rf, float s, float c, float pr, float pth,
+                               const Motion<float>& mo, float f[NV]) {
     rhs_separated<float>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f);
   }
 };
@@ -408,8 +458,8 @@ struct Ray {
   S h;       // proposed step (working type, like the reference's h)
   S h_taken; // step of the last accepted attempt
   double lam;
-  double m_null, m_q;
-  Refs ref;
+  typename M::D m_null, m_q;
+  Refs<typename M::D> ref;
   Trig tr;   // sin/cos of theta at y
   typename M::Shadow sh;
   long long attempts;
@@ -490,12 +540,13 @@ __device__ __forceinline__ void ray_init(const Params& P, const double y0[8], do
   const double fq = fe * fe * P.mass * P.mass;
   const double q_den = py_max(fabs(q0), fq);
   const double e_den = fe * fe;
+  using D = typename M::D;
   ry.ref.q0 = q0;
-  ry.ref.q_den = M::kFused ? 1.0 / q_den : q_den;
-  ry.ref.e_den = M::kFused ? 1.0 / e_den : e_den;
+  ry.ref.q_den = (D)(M::kFused ? 1.0 / q_den : q_den);
+  ry.ref.e_den = (D)(M::kFused ? 1.0 / e_den : e_den);
   M::init_rhs(P, ry.y, ry.pt, ry.pph, ry.sh, ry.f, ry.tr);
-  ry.m_null = drift<M>(null_error<M>(ry), ry.ref.e_den);
-  ry.m_q = 0.0;
+  ry.m_null = (D)drift<M>(null_error<M>(ry), (double)ry.ref.e_den);
+  ry.m_q = (D)0.0;
   ry.lam = 0.0;
   S h = (S)P.h0;
   if (!P.rk4 && (double)h > P.h_max) h = (S)P.h_max;
@@ -544,13 +595,14 @@ __device__ __forceinline__ typename M::N step_factor_sq(typename M::N en2, bool 
 }
 
 // The stages of one step of size h from ry.y with FSAL stage ry.f (numba_kernel.py:201-257):
-// k1..k5 (DP5; k1..k3 for RK4), the candidate state yn and k6 = f(yn).  With acc_rec, the
-// stage-input sums acc_s (stage input = y + h * acc_s) are recorded for s = 1..6 (the adjoint
-// rebuilds the stage inputs from them).
+// the candidate state yn, k6 = f(yn) and, for DP5, the error sum sum_i E_i k_i.  The solution
+// and error sums are accumulated in the reference's order of terms as soon as their stages are
+// known (the same values, fewer stages held live).  With acc_rec, the stage-input sums acc_s
+// (stage input = y + h * acc_s) are recorded for s = 1..6 (the adjoint rebuilds the stage
+// inputs from them).
 template <class M, bool RK4>
-__device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k1[NV],
-                                          typename M::K k2[NV], typename M::K k3[NV], typename M::K k4[NV],
-                                          typename M::K k5[NV], typename M::K k6[NV], typename M::S yn[NV], Trig& tr,
+__device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k6[NV],
+                                          typename M::S yn[NV], typename M::K esum[NV], Trig& tr,
                                           typename M::K (*acc_rec)[NV] = nullptr) {
   using K = typename M::K;
   const K* k0 = ry.f;
@@ -563,6 +615,7 @@ __device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typ
   // Stage inputs: the reference's sums (same terms and order, zero coefficients skipped);
   // madd fuses them in the fast modes and rounds each operation in the reference modes.
   if constexpr (!RK4) {
+    K k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], bsum[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = c(dp::A10) * k0[i];
     if (acc_rec) store(0);
@@ -586,17 +639,23 @@ __device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typ
     for (int i = 0; i < NV; ++i) {
       const K a = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
       acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::A52), k2[i]), c(dp::A53), k3[i]), c(dp::A54), k4[i]);
+      // b = (35/384, 0, 500/1113, 125/192, -2187/6784, 11/84) and E = b_hat - b through k4.
+      bsum[i] = madd<M>(madd<M>(madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]), c(dp::B3), k3[i]), c(dp::B4), k4[i]);
+      esum[i] = madd<M>(madd<M>(madd<M>(c(dp::E0) * k0[i], c(dp::E2), k2[i]), c(dp::E3), k3[i]), c(dp::E4), k4[i]);
     }
     if (acc_rec) store(4);
     M::template stage<false>(P, ry, h, acc, k5, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
-      const K a = madd<M>(c(dp::B0) * k0[i], c(dp::B2), k2[i]);
-      acc[i] = madd<M>(madd<M>(madd<M>(a, c(dp::B3), k3[i]), c(dp::B4), k4[i]), c(dp::B5), k5[i]);
+      acc[i] = madd<M>(bsum[i], c(dp::B5), k5[i]);
+      esum[i] = madd<M>(esum[i], c(dp::E5), k5[i]);
     }
     if (acc_rec) store(5);
     M::template stage<true>(P, ry, h, acc, k6, tr, yn);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) esum[i] = madd<M>(esum[i], c(dp::E6), k6[i]);
   } else {
+    K k1[NV], k2[NV], k3[NV];
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k0[i];
     if (acc_rec) store(0);
@@ -635,15 +694,19 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
   const bool last = (double)ry.h >= remaining;
   const S h_eff = last ? (S)remaining : ry.h;
   const K h = (K)h_eff;
-  K k1[NV], k2[NV], k3[NV], k4[NV], k5[NV], k6[NV];
+  K k6[NV], esum[NV];
   S yn[NV];
   Trig tr;
-  const K* k0 = ry.f;
-  auto c = [](double x) { return (K)x; };
-  dp_stages<M, RK4>(P, ry, h, k1, k2, k3, k4, k5, k6, yn, tr);
+  dp_stages<M, RK4>(P, ry, h, k6, yn, esum, tr);
+  // The candidate and k6 must be finite (numba_kernel.py:394-395).  In the fast DP5 modes the
+  // error norm decides it: every stage k_j except k1 enters sum E_j k_j (E_1 = 0, and k1 only
+  // feeds the later stages), yn derives from the same stages, and a non-finite yn makes its
+  // scale's Newton reciprocal NaN, so total is finite exactly when yn and k6 are.
   bool finite = true;
+  if constexpr (RK4 || !M::kFused) {
 #pragma unroll
-  for (int i = 0; i < NV; ++i) finite = finite && finite_(yn[i]) && finite_(k6[i]);
+    for (int i = 0; i < NV; ++i) finite = finite && finite_(yn[i]) && finite_(k6[i]);
+  }
   bool accept = finite;
   S h_new = ry.h;
   if constexpr (!RK4) {
@@ -655,10 +718,7 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
       N q[NV];
 #pragma unroll
       for (int i = 0; i < NV; ++i) {
-        K esum = madd<M>(c(dp::E0) * k0[i], c(dp::E2), k2[i]);
-        esum = madd<M>(madd<M>(madd<M>(madd<M>(esum, c(dp::E3), k3[i]), c(dp::E4), k4[i]), c(dp::E5), k5[i]),
-                       c(dp::E6), k6[i]);
-        const K e = h * esum;
+        const K e = h * esum[i];
         const N scale = madd<M>((N)P.atol, (N)P.rtol, py_max((N)fabs(ry.y[i]), (N)fabs(yn[i])));
         N v;
         if constexpr (M::kFused) v = (N)e * rcp_newton<1>(scale);
@@ -719,15 +779,16 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
     ry.y[i] = yn[i];
     ry.f[i] = k6[i];
   }
-  M::accepted(P, ry.y, ry.sh);
   ry.tr = M::accept_trig((double)ry.y[CTH], tr);
+  M::accepted(P, ry.y, ry.sh, ry.tr);
   const double lam_old = ry.lam;
   ry.lam = last ? P.lambda_max : ry.lam + (double)h_eff;
   ry.n_steps += 1;
   ry.h_taken = h_eff;
   // E and L_z drifts are identically zero (p_t, p_phi never change); Q and the null error:
-  ry.m_q = py_max(ry.m_q, drift<M>(fabs(carter<M>(P, ry) - ry.ref.q0), ry.ref.q_den));
-  ry.m_null = py_max(ry.m_null, drift<M>(null_error<M>(ry), ry.ref.e_den));
+  using D = typename M::D;
+  ry.m_q = py_max(ry.m_q, (D)drift<M>(fabs(carter<M>(P, ry) - ry.ref.q0), (double)ry.ref.q_den));
+  ry.m_null = py_max(ry.m_null, (D)drift<M>(null_error<M>(ry), (double)ry.ref.e_den));
   int code = classify<M>(P, ry, true, false);
   if (P.disk) {  // disk-plane event, numba_kernel.py:439-454
     const double half_pi = 0.5 * PI;
@@ -803,10 +864,10 @@ __device__ __forceinline__ void ray_store(const Ray<M>& ry, const Outputs& o, lo
   if (o.n_steps) o.n_steps[n] = ry.n_steps;
   if (o.n_rej) o.n_rej[n] = ry.n_rej;
   if (o.lam) o.lam[n] = ry.lam;
-  if (o.max_null) o.max_null[n] = ry.m_null;
+  if (o.max_null) o.max_null[n] = (double)ry.m_null;
   if (o.max_e) o.max_e[n] = 0.0;
   if (o.max_lz) o.max_lz[n] = 0.0;
-  if (o.max_q) o.max_q[n] = ry.m_q;
+  if (o.max_q) o.max_q[n] = (double)ry.m_q;
 }
 
 }  // namespace krr

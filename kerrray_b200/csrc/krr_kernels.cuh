@@ -12,6 +12,7 @@
 
 #include "krr_device.cuh"
 #include "krr_camera.cuh"
+#include "krr_radial.cuh"
 
 namespace krr {
 
@@ -36,7 +37,22 @@ struct Queue {
   int error;                      // KRR error code raised on the device, or 0
   int pad;
   unsigned long long flagged;     // photons appended to the re-trace list
+  unsigned long long t_first;     // globaltimer (ns) of the first block's start (PDL_STAMP), from ~0
+  unsigned long long t_last;      // globaltimer (ns) of the last block's end (PDL_STAMP)
 };
+
+// Programmatic dependent launch (sm_90+) of the persistent kernel, as bits of its `pdl`
+// argument: PDL_TRIGGER lets the next kernel of the stream launch (if it was launched as a
+// programmatic dependent) as soon as every block of this one has started; PDL_WAIT makes this
+// kernel, launched as such a dependent, wait at its exit for the kernel before it to complete
+// (so later work of the stream sees both); PDL_STAMP records the kernel's start and end times.
+enum : int { PDL_TRIGGER = 1, PDL_WAIT = 2, PDL_STAMP = 4 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Initial state of global photon g: a row of Y0, or the camera pixel of its image.
 __device__ __forceinline__ void photon_source(const Image* __restrict__ images, int img,
@@ -104,13 +120,26 @@ __global__ void k_trace_plain(Params P, const Image* __restrict__ images, int n_
 // Queue entries are global photon indices, or positions in `index` (a re-trace list) when it
 // is given; the number of entries is `total`, or *d_total when that is given (a count written
 // on the device by the kernel before, so the launch can sit in a captured graph).
+// risk (nullable, one byte per photon, from k_risk_prepass): RISK_CRITICAL photons are skipped
+// (retired unwritten: another kernel traces them), and a photon that ends within 1 % of its
+// affine or step budget is marked RISK_RECHECK (its class could depend on the last steps).
+// spread: a warp holds at most ceil(entries / warps) photons at a time, so a short queue is
+// shared by every warp of the grid instead of filling the first warps' lanes.
 template <class M, bool RK4, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_trace_persistent(const Image* __restrict__ images, int n_images, long long total,
                        const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q, int refill_threshold,
-                       const long long* __restrict__ index, const unsigned long long* __restrict__ d_total) {
+                       const long long* __restrict__ index, const unsigned long long* __restrict__ d_total,
+                       unsigned char* __restrict__ risk, int spread, int pdl) {
   constexpr unsigned FULL = 0xffffffffu;
+  if (pdl & PDL_TRIGGER) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  if ((pdl & PDL_STAMP) && threadIdx.x == 0) atomicMin(&q->t_first, global_ns());
   if (d_total) total = (long long)*d_total;
+  int cap = 32;
+  if (spread) {
+    const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+    cap = (int)min(32LL, max(1LL, (total + warps - 1) / warps));
+  }
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   Ray<M> ry;
@@ -120,34 +149,50 @@ __global__ void __launch_bounds__(MAXT, MINB)
   long long g = -1;
   int img = 0;
   // Lane statistics, added when a photon retires (every busy lane slot is one step attempt).
-  unsigned long long my_attempts = 0, my_accepted = 0;
-  unsigned my_iters = 0;
+  // 32-bit lane totals, flushed to the queue's 64-bit counters before they could wrap.
+  unsigned my_attempts = 0, my_accepted = 0, my_iters = 0;
   auto retire = [&]() {
     ray_store<M>(ry, o, g);
-    my_attempts += (unsigned long long)ry.attempts;
-    my_accepted += (unsigned long long)ry.n_steps;
+    if (risk && (ry.lam > 0.99 * images[img].P.lambda_max || ry.n_steps > 0.99 * (double)images[img].P.max_steps))
+      risk[g] = RISK_RECHECK;
+    const unsigned long long ra = (unsigned long long)ry.attempts;
+    if (ra >= (1ull << 30) || my_attempts >= (1u << 30)) {
+      atomicAdd(&q->attempts, ra + my_attempts);
+      atomicAdd(&q->busy_iters, ra + my_attempts);
+      atomicAdd(&q->accepted, (unsigned long long)ry.n_steps + my_accepted);
+      my_attempts = my_accepted = 0;
+    } else {
+      my_attempts += (unsigned)ra;
+      my_accepted += (unsigned)ry.n_steps;
+    }
     atomicAdd(&q->retired, 1ull);
   };
   while (true) {
     const unsigned idle = __ballot_sync(FULL, !active);
     const int n_idle = __popc(idle);
-    if (!drained && n_idle > 0 && (n_idle >= refill_threshold || n_idle == 32)) {
+    const int want = min(n_idle, cap - (32 - n_idle));
+    if (!drained && want > 0 && (n_idle >= refill_threshold || n_idle == 32)) {
       unsigned long long base = 0;
       const int leader = __ffs(idle) - 1;
-      if ((int)lane == leader) base = atomicAdd(&q->head, (unsigned long long)n_idle);
+      if ((int)lane == leader) base = atomicAdd(&q->head, (unsigned long long)want);
       base = __shfl_sync(FULL, base, leader);
-      if (base + (unsigned long long)n_idle >= (unsigned long long)total) drained = true;
-      if (!active) {
-        const unsigned long long mine = base + (unsigned long long)__popc(idle & lt_mask);
+      if (base + (unsigned long long)want >= (unsigned long long)total) drained = true;
+      const int rank = __popc(idle & lt_mask);
+      if (!active && rank < want) {
+        const unsigned long long mine = base + (unsigned long long)rank;
         if (mine < (unsigned long long)total) {
           g = index ? index[mine] : (long long)mine;
-          img = find_image(images, n_images, g);
-          const Image& im = images[img];
-          double y0[8];
-          photon_source(images, img, Y0, g, y0, q);
-          ray_init<M>(im.P, y0, carter_initial(im.P, y0), ry);
-          if (ry.state == RUNNING) active = true;
-          else retire();
+          if (risk && risk[g] == RISK_CRITICAL) {
+            atomicAdd(&q->retired, 1ull);  // traced by the reference-order kernel
+          } else {
+            img = find_image(images, n_images, g);
+            const Image& im = images[img];
+            double y0[8];
+            photon_source(images, img, Y0, g, y0, q);
+            ray_init<M>(im.P, y0, carter_initial(im.P, y0), ry);
+            if (ry.state == RUNNING) active = true;
+            else retire();
+          }
         }
       }
     }
@@ -169,17 +214,23 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
   }
   // Per-warp statistics (one atomic per counter per warp).
+  unsigned long long w_att = my_attempts, w_acc = my_accepted;
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
-    my_attempts += __shfl_down_sync(FULL, my_attempts, off);
-    my_accepted += __shfl_down_sync(FULL, my_accepted, off);
+    w_att += __shfl_down_sync(FULL, w_att, off);
+    w_acc += __shfl_down_sync(FULL, w_acc, off);
   }
   if (lane == 0) {
-    atomicAdd(&q->attempts, my_attempts);
-    atomicAdd(&q->accepted, my_accepted);
-    atomicAdd(&q->busy_iters, my_attempts);
+    atomicAdd(&q->attempts, w_att);
+    atomicAdd(&q->accepted, w_acc);
+    atomicAdd(&q->busy_iters, w_att);
     atomicAdd(&q->lane_iters, (unsigned long long)my_iters * 32ull);
   }
+  if (pdl & PDL_STAMP) {
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&q->t_last, global_ns());
+  }
+  if (pdl & PDL_WAIT) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // ------------------------------------------------------------------------------------------
@@ -368,6 +419,9 @@ struct PersistArgs {
   int block;
   const long long* index;             // re-trace list (nullable)
   const unsigned long long* d_total;  // device-side entry count (nullable)
+  unsigned char* risk;                // analytic classes (nullable): skip the critical photons
+  int spread;                         // share a short queue over every warp
+  int pdl;                            // PDL_* bits; with PDL_WAIT launched as a programmatic dependent
 };
 
 template <class M, bool RK4>
@@ -381,9 +435,18 @@ cudaError_t run_plain(const PlainArgs& a, int block, cudaStream_t s) {
 template <class M, bool RK4, int MAXT, int MINB>
 cudaError_t run_persistent(const PersistArgs& a, cudaStream_t s) {
   if (a.total <= 0 && !a.d_total) return cudaSuccess;
-  k_trace_persistent<M, RK4, MAXT, MINB><<<a.grid, MAXT, 0, s>>>(a.images, a.n_images, a.total, a.Y0, a.o, a.q,
-                                                                  a.refill_threshold, a.index, a.d_total);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)a.grid);
+  cfg.blockDim = dim3(MAXT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (a.pdl & PDL_WAIT) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k_trace_persistent<M, RK4, MAXT, MINB>, a.images, a.n_images, (long long)a.total,
+                            a.Y0, a.o, a.q, a.refill_threshold, a.index, a.d_total, a.risk, a.spread, a.pdl);
 }
 
 template <class M, bool RK4, int MAXT, int MINB>
@@ -416,6 +479,18 @@ constexpr Variant make_variant() {
   return Variant{MAXT, MINB, &run_persistent<M, RK4, MAXT, MINB>, &persistent_occupancy<M, RK4, MAXT, MINB>,
                  &persistent_registers<M, RK4, MAXT, MINB>};
 }
+
+// Analytic classes of every photon (krr_radial.cuh) into risk[]; the critical photons'
+// global indices are appended to `list` and counted in q->flagged.
+__global__ void k_risk_prepass(const Image* __restrict__ images, int n_images, long long total,
+                               const double* __restrict__ Y0, unsigned char* __restrict__ risk,
+                               long long* __restrict__ list, Queue* q);
+
+// After the traces: every non-critical photon whose code is not its analytic class, and with
+// `recheck` every photon marked RISK_RECHECK, is appended to `list` and counted in q->flagged.
+__global__ void k_check_risk(const Image* __restrict__ images, int n_images, long long total,
+                             const unsigned char* __restrict__ risk, const long long* __restrict__ state,
+                             long long* __restrict__ list, Queue* q, int recheck);
 
 template <class M, bool RK4>
 int plain_occupancy(int block) {

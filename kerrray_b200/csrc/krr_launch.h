@@ -45,6 +45,15 @@ cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s);
 cudaError_t flag_boundary(const Image* images, int n_images, long long total, const long long* state, long long* list,
                           Queue* q, cudaStream_t s);
 
+// The critical-set pipeline: analytic classes of every photon (critical ones appended to
+// `list`), the reference-order kernel whose blocks fill an SM each, and the check of the mixed
+// results against the analytic classes (disagreements appended to `list`).
+cudaError_t risk_prepass(const Image* images, int n_images, long long total, const double* Y0, unsigned char* risk,
+                         long long* list, Queue* q, cudaStream_t s);
+const Variant* ref_wide_variant();
+cudaError_t check_risk(const Image* images, int n_images, long long total, const unsigned char* risk,
+                       const long long* state, long long* list, Queue* q, bool recheck, cudaStream_t s);
+
 // Camera initial states for a pixel grid (alpha == beta == nullptr) or for points.
 cudaError_t camera_states(const Frame& F, double fov, long long res, const double* alpha, const double* beta,
                           long long n, double* Y0, int* err, cudaStream_t s);

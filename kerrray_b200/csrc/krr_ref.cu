@@ -22,9 +22,78 @@ const Variant* ref_variants(bool dtype32, bool rk4, int* count) {
 
 cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s) { return run_bisect<RefMode<double>, 128, 1>(a, s); }
 
+// Eight warps per block: at the reference order's register count one block fills an SM's
+// register file, so the critical photons of the mixed pipeline hold SMs of their own.
+const Variant* ref_wide_variant() {
+  static const Variant v = make_variant<RefMode<double>, false, 256, 1>();
+  return &v;
+}
+
+// Warp-aggregated append of the flagged lanes' global indices to list (count in q->flagged).
+__device__ __forceinline__ void append_flagged(bool flag, long long g, long long* list, Queue* q) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const unsigned mask = __ballot_sync(FULL, flag);
+  if (mask) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if ((int)lane == leader) base = atomicAdd(&q->flagged, (unsigned long long)__popc(mask));
+    base = __shfl_sync(FULL, base, leader);
+    if (flag) list[base + __popc(mask & ((1u << lane) - 1u))] = g;
+  }
+}
+
+__global__ void k_risk_prepass(const Image* __restrict__ images, int n_images, long long total,
+                               const double* __restrict__ Y0, unsigned char* __restrict__ risk,
+                               long long* __restrict__ list, Queue* q) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  bool critical = false;
+  if (g < total) {
+    const int img = find_image(images, n_images, g);
+    const Params& P = images[img].P;
+    double y0[8];
+    photon_source(images, img, Y0, g, y0, q);
+    const int cls = radial_risk(P.mass, P.a, P.r_capture, y0, risk_band(P.mass, P.rtol));
+    risk[g] = (unsigned char)cls;
+    critical = cls == RISK_CRITICAL;
+  }
+  append_flagged(critical, g, list, q);
+}
+
+__global__ void k_check_risk(const Image* __restrict__ images, int n_images, long long total,
+                             const unsigned char* __restrict__ risk, const long long* __restrict__ state,
+                             long long* __restrict__ list, Queue* q, int recheck) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  bool flag = false;
+  if (g < total) {
+    const int cls = risk[g];
+    const long long st = state[g];
+    if (cls == RISK_ESCAPE) flag = st != ESCAPED;
+    else if (cls == RISK_CAPTURE) flag = st != CAPTURED;
+    else if (cls == RISK_RECHECK) flag = recheck != 0;
+  }
+  append_flagged(flag, g, list, q);
+}
+
+cudaError_t risk_prepass(const Image* images, int n_images, long long total, const double* Y0, unsigned char* risk,
+                         long long* list, Queue* q, cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  const int block = 256;  // a multiple of 32: the append is warp-aggregated
+  k_risk_prepass<<<(unsigned)((total + block - 1) / block), block, 0, s>>>(images, n_images, total, Y0, risk, list, q);
+  return cudaGetLastError();
+}
+
+cudaError_t check_risk(const Image* images, int n_images, long long total, const unsigned char* risk,
+                       const long long* state, long long* list, Queue* q, bool recheck, cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  const int block = 256;
+  k_check_risk<<<(unsigned)((total + block - 1) / block), block, 0, s>>>(images, n_images, total, risk, state, list, q,
+                                                                        recheck ? 1 : 0);
+  return cudaGetLastError();
+}
+
 __global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, long long total,
                                 const long long* __restrict__ state, long long* __restrict__ list, Queue* q) {
-  constexpr unsigned FULL = 0xffffffffu;
   const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   bool flag = false;
   if (g < total) {
@@ -42,15 +111,7 @@ __global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, 
       }
     }
   }
-  const unsigned mask = __ballot_sync(FULL, flag);
-  if (mask) {
-    const unsigned lane = threadIdx.x & 31u;
-    const int leader = __ffs(mask) - 1;
-    unsigned long long base = 0;
-    if ((int)lane == leader) base = atomicAdd(&q->flagged, (unsigned long long)__popc(mask));
-    base = __shfl_sync(FULL, base, leader);
-    if (flag) list[base + __popc(mask & ((1u << lane) - 1u))] = g;
-  }
+  append_flagged(flag, g, list, q);
 }
 
 cudaError_t flag_boundary(const Image* images, int n_images, long long total, const long long* state, long long* list,

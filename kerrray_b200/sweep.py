@@ -26,7 +26,23 @@ from kerrray_b200 import _lib
 from kerrray_b200.camera import Camera
 from kerrray_b200.types import BatchResult, TerminationState
 
-__all__ = ["ImageSpec", "SweepResult", "DeviceSweep", "LaunchConfig", "order_by_cost", "trace_images"]
+__all__ = ["ImageSpec", "SweepResult", "DeviceSweep", "LaunchConfig", "order_by_cost", "trace_images", "RETRACE_EDGE",
+           "RETRACE_CRITICAL", "analytic_classes"]
+
+RETRACE_EDGE = 1
+RETRACE_CRITICAL = 2
+
+
+def analytic_classes(spacetime, y0: np.ndarray, rtol: float, horizon_epsilon: float = 1e-6) -> np.ndarray:
+    """Analytic class of each initial state (``krr_analytic_classes``): 0 escapes, 1 is captured,
+    2 lies within the critical band of the boundary (or is not classified)."""
+    y0 = np.ascontiguousarray(np.asarray(y0, dtype=np.float64))
+    if y0.ndim != 2 or y0.shape[1] != 8:
+        raise ValueError(f"Y0 must have shape (n, 8), got {y0.shape}")
+    out = np.empty(len(y0), dtype=np.uint8)
+    _lib.check(_lib.lib().krr_analytic_classes(float(spacetime.mass), float(spacetime.spin), float(rtol),
+                                               float(horizon_epsilon), _lib.ptr(y0), len(y0), _lib.ptr(out)))
+    return out
 
 
 @dataclass(frozen=True)
@@ -57,7 +73,11 @@ class LaunchConfig:
     refill_threshold: int = 0  # idle lanes before a warp refills (0 = 1)
     plain: bool = False       # one thread per photon instead of the work queue
     variant: int = 0          # compiled launch shape of the persistent kernel
-    retrace: bool = False     # re-trace edge and failed pixels with the reference-order FP64 kernel
+    # Settle the pixels a mixed trace could classify differently with the reference-order FP64
+    # kernel: 0 off; 1 (RETRACE_EDGE) afterwards, every pixel not ESCAPED or CAPTURED or unlike a
+    # neighbour; 2 (RETRACE_CRITICAL) the photons near the critical curve (analytic classes from
+    # the radial potential) beside the main trace, then every photon unlike its class.
+    retrace: int = 0
 
 
 def order_by_cost(specs: Sequence[ImageSpec]) -> list[int]:

@@ -268,7 +268,7 @@ def test_mixed_with_fp64_retrace_reproduces_the_plain_fp64_mask() -> None:
     """FP32 stages + FP64 re-trace of edge/failed pixels: the mask of the plain FP64 kernel, exactly."""
     specs = _spin99_specs(256)
     plain = K.trace_images(specs, precision="reference", launch=K.LaunchConfig(plain=True))
-    mixed = K.trace_images(specs, precision="mixed", launch=K.LaunchConfig(retrace=True))
+    mixed = K.trace_images(specs, precision="mixed", launch=K.LaunchConfig(retrace=K.RETRACE_EDGE))
     assert mixed.stats["retraced"] > 0 and mixed.stats["retired"] == mixed.stats["photons"]
     assert np.array_equal(mixed.arrays["state"], plain.arrays["state"])
     # The re-traced pixels carry exactly the plain kernel's FP64 results.
@@ -283,10 +283,35 @@ def test_mixed_with_fp64_retrace_reproduces_the_plain_fp64_mask() -> None:
           f"median {np.median(rel):.2e}")
 
 
+def test_mixed_with_critical_set_reproduces_the_plain_fp64_mask() -> None:
+    """FP32 stages + the analytic critical set traced in reference-order FP64 beside them (and a
+    re-trace of anything unlike its analytic class): the plain FP64 kernel's mask, exactly."""
+    specs = _spin99_specs(256)
+    plain = K.trace_images(specs, precision="reference", launch=K.LaunchConfig(plain=True))
+    mixed = K.trace_images(specs, precision="mixed", launch=K.LaunchConfig(retrace=K.RETRACE_CRITICAL))
+    st = mixed.stats
+    assert st["critical"] > 0 and st["retired"] == st["photons"]
+    assert st["retraced"] == st["critical"] + st["rechecked"]
+    assert np.array_equal(mixed.arrays["state"], plain.arrays["state"])
+    # The critical photons carry the plain kernel's FP64 results bit for bit.
+    y0 = np.concatenate([K.initial_states(s.camera, s.spacetime) for s in specs])
+    cls = np.concatenate([K.analytic_classes(s.spacetime, y0[mixed.rows(k)], s.integ.rtol)
+                          for k, s in enumerate(specs)])
+    crit = np.flatnonzero(cls == 2)
+    assert crit.size == st["critical"]
+    assert np.array_equal(mixed.arrays["Y"][crit], plain.arrays["Y"][crit])
+    assert np.array_equal(mixed.arrays["n_steps"][crit], plain.arrays["n_steps"][crit])
+    # Every non-critical photon ended in its analytic class.
+    codes = mixed.arrays["state"]
+    assert np.all(codes[cls == 0] == 1) and np.all(codes[cls == 1] == 2)
+    print(f"critical set: {st['critical']} critical, {st['rechecked']} rechecked of {st['photons']}")
+
+
 def test_captured_graph_plan_equals_direct_launch() -> None:
     torch = pytest.importorskip("torch")
     specs = _spin99_specs(128)
-    for precision, retrace in (("fast64", False), ("mixed", True), ("reference", False)):
+    for precision, retrace in (("fast64", 0), ("mixed", K.RETRACE_EDGE), ("mixed", K.RETRACE_CRITICAL),
+                               ("reference", 0)):
         cfg = K.LaunchConfig(retrace=retrace)
         direct = K.trace_images(specs, precision=precision, launch=cfg)
         sw = K.DeviceSweep(specs, precision=precision, launch=cfg, graph=True)
