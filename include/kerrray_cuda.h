@@ -136,7 +136,8 @@ typedef struct krr_launch {
   int32_t retrace;           /* KRR_RETRACE_*: settle the pixels a mixed trace could classify
                                 differently with the reference-order FP64 kernel (rk45, float64,
                                 persistent launches) */
-  int32_t reserved;
+  int32_t critical_sms;      /* KRR_RETRACE_CRITICAL: SMs of the critical-set kernel (0: 1/37 of
+                                the SMs, at least 2) */
 } krr_launch;
 
 /* A compiled launch shape of the persistent kernel: threads per block and the launch-bounds

@@ -71,7 +71,7 @@ class KrrEdgeCase(ctypes.Structure):
 class KrrLaunch(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("refill_threshold", ctypes.c_int32), ("plain", ctypes.c_int32), ("variant", ctypes.c_int32),
-                ("retrace", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("retrace", ctypes.c_int32), ("critical_sms", ctypes.c_int32)]
 
 
 class KrrVariantInfo(ctypes.Structure):

@@ -3,10 +3,12 @@
 Chooses, for a list of images and a precision, the compiled launch variant (threads per block
 and register cap, i.e. how many warps stay resident per SM) and the refill threshold (how many
 lanes of a warp may sit idle before the warp pulls new photons from the queue) by timing
-each candidate on a reduced copy of the workload: the same images at a quarter of the
+each candidate on a reduced copy of the workload: the same images at a half or a quarter of the
 resolution per side (same field of view, so the same mix of escaping, captured and
-near-critical photons). Each warp handles 32 photons at a time, one per lane; the refill
-claims as many queue entries as the warp has idle lanes.
+near-critical photons), reduced only while at least half a million photons remain -- fewer
+leave the launch's tail in charge and favour other shapes than the full workload would. Each
+warp handles 32 photons at a time, one per lane; the refill claims as many queue entries as
+the warp has idle lanes.
 
 Results are cached per device, precision and workload signature in memory and, when
 ``KRR_AUTOTUNE_CACHE`` names a file, in that JSON file.
@@ -78,10 +80,25 @@ def _save_file(table: dict) -> None:
         Path(path).write_text(json.dumps(table, indent=1))
 
 
-def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: int = 0, scale: int = 4,
+MIN_TUNING_PHOTONS = 500_000
+
+
+def tuning_scale(specs: Sequence[ImageSpec]) -> int:
+    """Largest reduction per side in (4, 2, 1) that keeps MIN_TUNING_PHOTONS photons."""
+    total = sum(s.n_rays for s in specs)
+    for scale in (4, 2):
+        if total // (scale * scale) >= MIN_TUNING_PHOTONS:
+            return scale
+    return 1
+
+
+def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: int = 0, scale: int | None = None,
              thresholds: Sequence[int] = (1, 4, 8, 16), repeats: int = 2, use_cache: bool = True) -> tuple[LaunchConfig, dict]:
-    """Return the fastest ``LaunchConfig`` for ``specs`` and a report of every candidate's time."""
+    """Return the fastest ``LaunchConfig`` for ``specs`` and a report of every candidate's time
+    (``scale``: reduction per side of the tuning workload; None chooses ``tuning_scale``)."""
     specs = list(specs)
+    if scale is None:
+        scale = tuning_scale(specs)
     key = _signature(specs, precision, device)
     if use_cache:
         if key in _CACHE:
@@ -91,7 +108,7 @@ def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: i
         if key in table:
             _CACHE[key] = table[key]
             return LaunchConfig(**table[key]["config"]), table[key]
-    small = _reduced(specs, scale)
+    small = _reduced(specs, scale) if scale > 1 else specs
     variants = list_variants(precision, specs[0].integ, specs[0].term, device)
     trials = []
     best = None
@@ -108,7 +125,7 @@ def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: i
                 best = (cfg, ms)
             del sweep
     report = {"config": {"variant": best[0].variant, "refill_threshold": best[0].refill_threshold},
-              "ms": best[1], "photons": sum(s.n_rays for s in small), "trials": trials}
+              "ms": best[1], "photons": sum(s.n_rays for s in small), "scale": scale, "trials": trials}
     _CACHE[key] = report
     if use_cache and os.environ.get("KRR_AUTOTUNE_CACHE"):
         table = _load_file()

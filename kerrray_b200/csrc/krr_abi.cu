@@ -490,19 +490,19 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     p.re.d_total = &p.w.q0->flagged;
   }
   if (p.retrace_mode == KRR_RETRACE_CRITICAL) {
-    // The reference-order kernel takes the critical photons on 1/18 of the SMs: launched first,
+    // The reference-order kernel takes the critical photons on a few SMs: launched first,
     // each of its blocks fills an SM's register file, and it lets the main (mixed) trace launch
     // as soon as its blocks run (programmatic dependent launch), so the main trace -- which
     // skips the critical photons -- spreads over the other SMs and the two run side by side.
-    // The main trace waits for it only at its exit.  Afterwards the photons unlike their
-    // analytic class are traced again in fast FP64, and what still disagrees (or ended near
-    // its budget) in reference order.
+    // The main trace keeps its full grid: the blocks that do not fit wait for the critical
+    // kernel's SMs and join the work queue when its blocks exit.  It waits for the critical
+    // kernel only at its own exit.  Afterwards the photons unlike their analytic class are
+    // traced again in fast FP64, and what still disagrees (or ended near its budget) in
+    // reference order.
     const krr::Variant* wv = krr::ref_wide_variant();
     if (wv->occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "the critical-set kernel cannot be resident");
     const int sms = std::max(sm_count_of(device), 2);
-    const int crit_sms = std::max(1, sms / 18);
-    const int bps = std::max(1, p.main.grid / sms);
-    p.main.grid = (sms - crit_sms) * bps;
+    const int crit_sms = std::min(sms - 1, (launch && launch->critical_sms > 0) ? launch->critical_sms : std::max(2, sms / 37));
     p.main.risk = p.w.risk;
     p.main.pdl = krr::PDL_WAIT;
     p.crit = p.main;

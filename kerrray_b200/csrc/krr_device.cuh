@@ -24,6 +24,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace krr {
@@ -259,20 +260,11 @@ __device__ __forceinline__ double rcp_fast(double x) { return rcp_newton<2>(x); 
 __device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
 
 // sin and cos of theta0 + d from s0 = sin(theta0), c0 = cos(theta0) by the angle-addition
-// formulas, with sin d and cos d from their Taylor series: through d^7 and d^6 in FP32
-// (|d| <= 1/4: truncation below 4e-10), through d^9 and d^10 in FP64 (|d| <= 1/10: below
-// 3e-19).  The stages of one step move theta by such small amounts, so this replaces a full
-// sincos (argument reduction and two polynomials) by about a dozen fused operations.
-// Returns false, computing nothing, when |d| exceeds the range.
-__device__ __forceinline__ bool sincos_shift(float s0, float c0, float d, float& s, float& c) {
-  if (!(fabsf(d) <= 0.25f)) return false;
-  const float d2 = d * d;
-  const float sd = d * fmaf(d2, fmaf(d2, fmaf(d2, -1.0f / 5040.0f, 1.0f / 120.0f), -1.0f / 6.0f), 1.0f);
-  const float cd = fmaf(d2, fmaf(d2, fmaf(d2, -1.0f / 720.0f, 1.0f / 24.0f), -0.5f), 1.0f);
-  s = fmaf(s0, cd, c0 * sd);
-  c = fmaf(c0, cd, -(s0 * sd));
-  return true;
-}
+// formulas, with sin d and cos d from their Taylor series: through d^9 and d^10 in FP64
+// (|d| <= 1/10: truncation below 3e-19); the FP32 form (sincos_shift_x2) goes through d^7 and
+// d^6 (|d| <= 1/4: below 4e-10).  The stages of one step move theta by such small amounts, so
+// this replaces a full sincos (argument reduction and two polynomials) by about a dozen fused
+// operations.  Returns false, computing nothing, when |d| exceeds the range.
 __device__ __forceinline__ bool sincos_shift(double s0, double c0, double d, double& s, double& c) {
   if (!(fabs(d) <= 0.1)) return false;
   const double d2 = d * d;
@@ -322,6 +314,27 @@ __device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth,
   f[CPR] = isig * fused(r, bs, -fused(rm, pr2, kd * fused(kd, rm, mo.m2e * r)));
   // -dH/dtheta = cos (v (L / sin^2 + a E) - a^2 sin B / Sigma) / Sigma
   f[CPTH] = (isig * c) * fused(v, fused(lis, is, mo.ae), -(a2 * s) * bs);
+}
+
+// The FP32 sincos_shift on packed pairs (fma/mul.rn.f32x2, sm_100): the sine and cosine
+// polynomials and the two rotation products advance together, every value the same operation
+// on the same operands as in the scalar form.  (The right-hand side stays scalar: packing its
+// operands ties registers into pairs, and the moves cost more than the instructions saved.)
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+__device__ __forceinline__ bool sincos_shift_x2(float s0, float c0, float d, float& s, float& c) {
+  if (!(fabsf(d) <= 0.25f)) return false;
+  const float d2 = d * d;
+  const float2 dd = f2(d2, d2);
+  float2 p = __ffma2_rn(dd, f2(-1.0f / 5040.0f, -1.0f / 720.0f), f2(1.0f / 120.0f, 1.0f / 24.0f));
+  p = __ffma2_rn(dd, p, f2(-1.0f / 6.0f, -0.5f));
+  p = __ffma2_rn(dd, p, f2(1.0f, 1.0f));  // (sin d / d, cos d)
+  const float sd = d * p.x;
+  const float2 t = __fmul2_rn(f2(c0, -s0), f2(sd, sd));
+  const float2 r = __ffma2_rn(f2(s0, c0), f2(p.y, p.y), t);
+  s = r.x;
+  c = r.y;
+  return true;
 }
 
 // FP64 with explicit FMAs, sincos and Newton reciprocals on the separated form.
@@ -391,10 +404,11 @@ struct Mixed {
   using D = float;
   static constexpr bool kFused = true;
 
-  // FP32 copy of what the stages read: r - r_plus, r, theta with its sine and cosine, p_r,
-  // p_theta, and the ray's constants of motion.
+  // FP32 copy of what the stages read: (r, r - r_plus), (p_r, p_theta) as packed pairs, theta
+  // with its sine and cosine, and the ray's constants of motion.
   struct Shadow {
-    float d0, r, th, s0, c0, pr, pth;
+    float2 rd, pp;
+    float th, s0, c0;
     Motion<float> mo;
   };
 
@@ -407,36 +421,36 @@ struct Mixed {
 
   // tr: the accepted state's FP64 sine and cosine (accept_trig).
   __device__ static void accepted(const Params& P, const S y[NV], Shadow& sh, const Trig& tr) {
-    sh.d0 = (float)(y[CR] - P.r_plus);
-    sh.r = (float)y[CR];
+    sh.rd = make_float2((float)y[CR], (float)(y[CR] - P.r_plus));
+    sh.pp = make_float2((float)y[CPR], (float)y[CPTH]);
     sh.th = (float)y[CTH];
     sh.s0 = (float)tr.s;
     sh.c0 = (float)tr.c;
-    sh.pr = (float)y[CPR];
-    sh.pth = (float)y[CPTH];
   }
 
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow& sh, K f[NV], Trig& tr) {
     sh.mo.set((float)pt, (float)pph, (float)P.a);
     tr = accept_trig(y[CTH], tr);
     accepted(P, y, sh, tr);
-    rhs_f(P, sh.d0, sh.r, sh.s0, sh.c0, sh.pr, sh.pth, sh.mo, f);
+    rhs_f(P, sh.rd.y, sh.rd.x, sh.s0, sh.c0, sh.pp.x, sh.pp.y, sh.mo, f);
   }
 
+  // The right-hand side at the stage input shadow + h * acc, from the pairs (r, theta) and
+  // (p_r, p_theta) of acc; k receives f as the pairs (r, theta), (p_r, p_theta), (t, phi).
   // Every stage's sine and cosine come from the accepted state's by a small-angle shift; near
   // the axis (|sin| < 1/50, where the shift's sum would cancel) or for a large shift, sincosf.
-  template <bool LAST, class R>
-  __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig&, S yn[NV]) {
-    const Shadow& sh = ry.sh;
-    const float dth = h * acc[CTH];
+  __device__ static void stage(const Params& P, const Shadow& sh, float h, const float2 acc[2], float2 k[3]) {
+    const float2 hh = make_float2(h, h);
+    const float2 rd = __ffma2_rn(hh, make_float2(acc[0].x, acc[0].x), sh.rd);  // (r, r - r_plus)
+    const float2 pp = __ffma2_rn(hh, acc[1], sh.pp);                           // (p_r, p_theta)
+    const float dth = h * acc[0].y;
     float s, c;
-    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift(sh.s0, sh.c0, dth, s, c))) sincosf(sh.th + dth, &s, &c);
-    rhs_f(P, fmaf(h, acc[CR], sh.d0), fmaf(h, acc[CR], sh.r), s, c, fmaf(h, acc[CPR], sh.pr), fmaf(h, acc[CPTH], sh.pth),
-          sh.mo, f);
-    if constexpr (LAST) {
-#pragma unroll
-      for (int i = 0; i < NV; ++i) yn[i] = ry.y[i] + (double)(h * acc[i]);  // FP64 accumulation
-    }
+    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift_x2(sh.s0, sh.c0, dth, s, c))) sincosf(sh.th + dth, &s, &c);
+    float f[NV];
+    rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, f);
+    k[0] = make_float2(f[CR], f[CTH]);
+    k[1] = make_float2(f[CPR], f[CPTH]);
+    k[2] = make_float2(f[CT], f[CPH]);
   }
 
   // The right-hand side in FP32 at (r - r_plus = d, r, sin, cos, p_r, p_theta).
@@ -601,7 +615,7 @@ __device__ __forceinline__ typename M::N step_factor_sq(typename M::N en2, bool 
 // (stage input = y + h * acc_s) are recorded for s = 1..6 (the adjoint rebuilds the stage
 // inputs from them).
 template <class M, bool RK4>
-__device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k6[NV],
+__device__ __forceinline__ void dp_stages_scalar(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k6[NV],
                                           typename M::S yn[NV], typename M::K esum[NV], Trig& tr,
                                           typename M::K (*acc_rec)[NV] = nullptr) {
   using K = typename M::K;
@@ -674,6 +688,91 @@ __device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typ
                        c(dp::RK4_B3), k3[i]);
     if (acc_rec) store(5);
     M::template stage<true>(P, ry, h, acc, k6, tr, yn);
+  }
+}
+
+// The mixed mode's stages on packed FP32 pairs.  sm_100 executes two FP32 multiply-adds in one
+// instruction (fma.rn.f32x2); with the components paired as (r, theta), (p_r, p_theta) and
+// (t, phi), each stage sum takes one packed operation per pair where the scalar form takes
+// two.  Every lane rounds exactly like the scalar operation and the sums keep the reference's
+// order of terms, so the values are those of the scalar form.  Only the pairs the right-hand
+// side reads are formed for the inner stages; (t, phi) enters the solution and error sums.
+__device__ __forceinline__ float2 mul2(float a, float2 x) { return __fmul2_rn(make_float2(a, a), x); }
+__device__ __forceinline__ float2 madd2(float2 acc, float a, float2 x) { return __ffma2_rn(make_float2(a, a), x, acc); }
+
+__device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<Mixed>& ry, float h, float k6[NV],
+                                                double yn[NV], float esum[NV]) {
+  auto c = [](double x) { return (float)x; };
+  const Mixed::Shadow& sh = ry.sh;
+  float2 k0[3], k1[3], k2[3], k3[3], k4[3], k5[3], kl[3], acc[3], bs[3], es[3];
+  k0[0] = make_float2(ry.f[CR], ry.f[CTH]);
+  k0[1] = make_float2(ry.f[CPR], ry.f[CPTH]);
+  k0[2] = make_float2(ry.f[CT], ry.f[CPH]);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) acc[j] = mul2(c(dp::A10), k0[j]);
+  Mixed::stage(P, sh, h, acc, k1);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) acc[j] = madd2(mul2(c(dp::A20), k0[j]), c(dp::A21), k1[j]);
+  Mixed::stage(P, sh, h, acc, k2);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) acc[j] = madd2(madd2(mul2(c(dp::A30), k0[j]), c(dp::A31), k1[j]), c(dp::A32), k2[j]);
+  Mixed::stage(P, sh, h, acc, k3);
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+    acc[j] = madd2(madd2(madd2(mul2(c(dp::A40), k0[j]), c(dp::A41), k1[j]), c(dp::A42), k2[j]), c(dp::A43), k3[j]);
+  Mixed::stage(P, sh, h, acc, k4);
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+    acc[j] = madd2(madd2(madd2(madd2(mul2(c(dp::A50), k0[j]), c(dp::A51), k1[j]), c(dp::A52), k2[j]), c(dp::A53), k3[j]),
+                   c(dp::A54), k4[j]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    bs[j] = madd2(madd2(madd2(mul2(c(dp::B0), k0[j]), c(dp::B2), k2[j]), c(dp::B3), k3[j]), c(dp::B4), k4[j]);
+    es[j] = madd2(madd2(madd2(mul2(c(dp::E0), k0[j]), c(dp::E2), k2[j]), c(dp::E3), k3[j]), c(dp::E4), k4[j]);
+  }
+  Mixed::stage(P, sh, h, acc, k5);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    acc[j] = madd2(bs[j], c(dp::B5), k5[j]);
+    es[j] = madd2(es[j], c(dp::E5), k5[j]);
+  }
+  Mixed::stage(P, sh, h, acc, kl);
+  float2 ha[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    es[j] = madd2(es[j], c(dp::E6), kl[j]);
+    ha[j] = mul2(h, acc[j]);
+  }
+  // The candidate: h * acc rounded in FP32, accumulated into the FP64 state.
+  yn[CR] = ry.y[CR] + (double)ha[0].x;
+  yn[CTH] = ry.y[CTH] + (double)ha[0].y;
+  yn[CPR] = ry.y[CPR] + (double)ha[1].x;
+  yn[CPTH] = ry.y[CPTH] + (double)ha[1].y;
+  yn[CT] = ry.y[CT] + (double)ha[2].x;
+  yn[CPH] = ry.y[CPH] + (double)ha[2].y;
+  k6[CR] = kl[0].x;
+  k6[CTH] = kl[0].y;
+  k6[CPR] = kl[1].x;
+  k6[CPTH] = kl[1].y;
+  k6[CT] = kl[2].x;
+  k6[CPH] = kl[2].y;
+  esum[CR] = es[0].x;
+  esum[CTH] = es[0].y;
+  esum[CPR] = es[1].x;
+  esum[CPTH] = es[1].y;
+  esum[CT] = es[2].x;
+  esum[CPH] = es[2].y;
+}
+
+template <class M, bool RK4>
+__device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k6[NV],
+                                          typename M::S yn[NV], typename M::K esum[NV], Trig& tr,
+                                          typename M::K (*acc_rec)[NV] = nullptr) {
+  if constexpr (std::is_same<M, Mixed>::value) {
+    static_assert(!RK4, "the mixed mode integrates with Dormand-Prince 5(4) only");
+    dp_stages_mixed(P, ry, h, k6, yn, esum);
+  } else {
+    dp_stages_scalar<M, RK4>(P, ry, h, k6, yn, esum, tr, acc_rec);
   }
 }
 

@@ -78,6 +78,7 @@ class LaunchConfig:
     # neighbour; 2 (RETRACE_CRITICAL) the photons near the critical curve (analytic classes from
     # the radial potential) beside the main trace, then every photon unlike its class.
     retrace: int = 0
+    critical_sms: int = 0     # RETRACE_CRITICAL: SMs of the reference-order kernel (0: library default)
 
 
 def order_by_cost(specs: Sequence[ImageSpec]) -> list[int]:
@@ -103,7 +104,7 @@ def _launch(precision: str, cfg: LaunchConfig | None) -> _lib.KrrLaunch:
     cfg = cfg or LaunchConfig()
     return _lib.KrrLaunch(precision=_lib.PRECISIONS[precision], block=cfg.block, blocks_per_sm=cfg.blocks_per_sm,
                           refill_threshold=cfg.refill_threshold, plain=int(cfg.plain), variant=cfg.variant,
-                          retrace=int(cfg.retrace), reserved=0)
+                          retrace=int(cfg.retrace), critical_sms=int(cfg.critical_sms))
 
 
 @dataclass

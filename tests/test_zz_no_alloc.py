@@ -54,7 +54,7 @@ def test_noalloc_entry_point_matches_the_workspace_entry_point_twice() -> None:
     stream = torch.cuda.current_stream().cuda_stream
     for precision in ("fast64", "mixed"):
         launch = _lib.KrrLaunch(precision=_lib.PRECISIONS[precision], block=0, blocks_per_sm=0, refill_threshold=0,
-                                plain=0, variant=0, retrace=0)
+                                plain=0, variant=0, retrace=0, critical_sms=0)
         ref = _outputs(torch, total)
         ws = torch.zeros(int(L.krr_workspace_size(len(specs), 0)), dtype=torch.uint8, device="cuda")
         st = _lib.KrrStats()
