@@ -217,9 +217,11 @@ KRR_API int krr_trace_images_device(int device, const krr_image* images, int32_t
                             const krr_launch* launch, const krr_result* d_out, void* workspace,
                             size_t workspace_bytes, void* stream, krr_stats* stats);
 
-/* A batched launch captured once as a CUDA graph and replayed: krr_plan_create uploads the
- * image descriptors into `workspace` (krr_workspace_size bytes, caller-owned, like the outputs
- * and d_Y0 it must outlive the plan) and captures the whole launch sequence (counter resets,
+/* A batched launch captured once as a CUDA graph and replayed: krr_plan_create waits for the
+ * device to finish its pending work (so a workspace still being filled on another stream is
+ * safe), uploads the image descriptors into `workspace` (krr_workspace_size bytes,
+ * caller-owned, like the outputs and d_Y0 it must outlive the plan) and captures the whole
+ * launch sequence (counter resets,
  * persistent trace, and with retrace the flagging and FP64 re-trace, whose size is read on the
  * device); krr_plan_launch enqueues it on `stream` without synchronising; krr_plan_stats
  * synchronises `stream` and reads the counters of the last launch (kernel times 0: time the

@@ -863,6 +863,10 @@ int krr_plan_create(int device, const krr_image* images, int32_t n_images, const
   pl->device = device;
   rc = prepare_pipeline(device, images, n_images, total, d_Y0, launch, d_out, workspace, workspace_bytes, pl->p);
   if (rc) return rc;
+  // The caller may still be filling `workspace` (or the outputs) on a stream of its own -- e.g.
+  // the asynchronous zero fill of a freshly allocated buffer: wait for the device before the
+  // upload, which goes through this library's stream and is ordered after nothing else.
+  KRR_CUDA(cudaDeviceSynchronize());
   KRR_CUDA(cudaMemcpyAsync(pl->p.w.images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, c->stream));
   KRR_CUDA(cudaStreamSynchronize(c->stream));
   KRR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));

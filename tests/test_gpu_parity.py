@@ -324,6 +324,24 @@ def test_captured_graph_plan_equals_direct_launch() -> None:
         sw.close()
 
 
+def test_plan_creation_waits_for_a_workspace_still_being_filled() -> None:
+    """krr_plan_create uploads the image table on its own stream: a workspace whose zero fill is
+    still queued on the caller's stream (behind ~50 ms of other work) must not overwrite it."""
+    torch = pytest.importorskip("torch")
+    specs = _spin99_specs(128)
+    direct = K.trace_images(specs, precision="fast64")
+    # Leave blocks of these sizes in torch's cache, so that the sweep below reuses them without a
+    # (device-synchronising) cudaMalloc and their zero fill is an asynchronous kernel.
+    K.DeviceSweep(specs, precision="fast64", graph=False).close()
+    torch.cuda.synchronize()
+    torch.cuda._sleep(100_000_000)  # the caller's stream stays busy; the fill below queues behind it
+    sw = K.DeviceSweep(specs, precision="fast64", graph=True)
+    st = sw.run()
+    assert st["retired"] == st["photons"]
+    assert np.array_equal(sw.tensors["state"].cpu().numpy(), direct.arrays["state"])
+    sw.close()
+
+
 @pytest.mark.parametrize("name", ["edge_bisection_a0.9_rtol1e-06", "edge_bisection_a0_rtol1e-08"])
 def test_edge_bisection_matches_reference(name: str) -> None:
     """Device bisection (study_edge_bisection.py:53-68): same edge as the reference to ~rtol."""
