@@ -56,8 +56,12 @@ class EdgeCase:
 
 
 def bisect_edges(cases: Sequence[EdgeCase], iterations: int, *, precision: str = "reference",
-                 device: int = 0) -> tuple[list[tuple[np.ndarray, np.ndarray, int]], dict]:
-    """Run every case's bisection in one launch; per case ``(r_mid, width, failures)`` and the stats."""
+                 device: int = 0, item_failures: bool = False) -> tuple[list[tuple[np.ndarray, np.ndarray, object]], dict]:
+    """Run every case's bisection in one launch; per case ``(r_mid, width, failures)`` and the stats.
+
+    ``failures`` counts the photons of the case that ended neither ESCAPED nor CAPTURED (the
+    reference's lost photons); with ``item_failures`` it is that count per direction (an array).
+    """
     cases = list(cases)
     arr = (_lib.KrrEdgeCase * len(cases))(*[c.struct() for c in cases])
     sizes = [np.asarray(c.angles).size for c in cases]
@@ -80,7 +84,7 @@ def bisect_edges(cases: Sequence[EdgeCase], iterations: int, *, precision: str =
     start = 0
     for n in sizes:
         sl = slice(start, start + n)
-        out.append((0.5 * (lo[sl] + hi[sl]), hi[sl] - lo[sl], int(fails[sl].sum())))
+        out.append((0.5 * (lo[sl] + hi[sl]), hi[sl] - lo[sl], fails[sl].copy() if item_failures else int(fails[sl].sum())))
         start += n
     return out, stats.as_dict()
 
@@ -111,10 +115,13 @@ def edge_study(st, incl: float, r_o: float, rtol: float, angles, *, bracket: tup
     return EdgeCase(st, incl, r_o, rtol, (c_ana[0] / k, c_ana[1] / k), angles, lo, hi)
 
 
-def edge_error(case: EdgeCase, r_mid: np.ndarray, n_curve: int = 40000) -> dict[str, float]:
-    """Edge error against Bardeen's curve after the finite-distance correction (M)."""
+def edge_error(case: EdgeCase, r_mid: np.ndarray, n_curve: int = 40000, keep: np.ndarray | None = None) -> dict[str, float]:
+    """Edge error against Bardeen's curve after the finite-distance correction (M), over the
+    directions selected by ``keep`` (a boolean mask; all by default)."""
     k = finite_distance_scale(case.spacetime, case.r_o)
     ca, cb = analytic_boundary(case.spacetime, case.inclination_deg, n_curve)
     r_ana = polygon_radii(ca, cb, (case.centre[0] * k, case.centre[1] * k), case.angles)
     err = r_mid * k - r_ana
+    if keep is not None:
+        err = err[np.asarray(keep, dtype=bool)]
     return {"rms_M": float(np.sqrt(np.mean(err**2))), "max_M": float(np.max(np.abs(err))), "mean_M": float(np.mean(err))}
