@@ -514,19 +514,24 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     p.crit.index = p.w.list;
     p.crit.d_total = &p.w.q1->flagged;
     p.crit.risk = nullptr;
-    p.crit.spread = 1;
+    p.crit.flags = krr::TRACE_SPREAD;
     p.crit.pdl = krr::PDL_TRIGGER | krr::PDL_STAMP;
+    // Photons unlike their analytic class: after a mixed trace, rays an FP32 overflow ended
+    // early, traced again with the overflow taken as a rejection (MixedSat); otherwise in FP64.
     int nf = 0;
     const krr::Variant* fv = krr::fast_variants(false, false, &nf);
-    if (!fv || nf < 1 || fv[0].occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "no FP64 re-trace kernel");
-    p.fix_v = &fv[0];
+    if (!fv || nf < 1) return fail(KRR_ERR_UNSUPPORTED, "no FP64 re-trace kernel");
+    p.fix_v = (precision == KRR_PREC_MIXED) ? krr::mixed_sat_variant() : &fv[0];
+    if (p.fix_v->occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "the re-trace kernel cannot be resident");
     p.fix = p.crit;
     p.fix.q = p.w.q2;
-    p.fix.grid = sms * fv[0].occupancy();
-    p.fix.block = fv[0].block;
+    p.fix.grid = sms * p.fix_v->occupancy();
+    p.fix.block = p.fix_v->block;
     p.fix.d_total = &p.w.q2->flagged;
     p.fix.pdl = 0;
+    if (precision == KRR_PREC_MIXED) p.fix.flags |= krr::TRACE_RESUME;  // continue where the overflow stopped it
     p.re = p.fix;
+    p.re.flags = krr::TRACE_SPREAD;  // from the camera: the plain kernel's exact arithmetic
     p.re.q = p.w.q3;
     p.re.grid = sms * p.re_v->occupancy();
     p.re.block = p.re_v->block;

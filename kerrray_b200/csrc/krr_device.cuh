@@ -142,6 +142,8 @@ struct RefMode {
   using K = W;       // stage type
   using N = W;       // error-norm type
   using D = double;  // diagnostics (running maxima and their denominators)
+  static constexpr bool kSaturate = false;
+  static constexpr bool kMixed = false;
   static constexpr bool kFused = false;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
@@ -343,6 +345,8 @@ struct Fast64 {
   using K = double;
   using N = double;
   using D = float;  // the drift maxima: FP64 values, kept to single precision
+  static constexpr bool kSaturate = false;
+  static constexpr bool kMixed = false;
   static constexpr bool kFused = true;
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
@@ -402,6 +406,13 @@ struct Mixed {
   using K = float;
   using N = double;
   using D = float;
+  static constexpr bool kMixed = true;
+  // A trial step through the singular region can overflow the FP32 stages where FP64 stays
+  // finite (values of 1e13..1e40 near r_+), and FP64 then rejects it with the smallest step
+  // factor because its error norm is huge.  This mode ends such a ray as a NUMERICAL_FAILURE
+  // like the reference does on a non-finite step (a handful of rays per million; the
+  // pipelines trace them again); MixedSat below rejects instead.
+  static constexpr bool kSaturate = false;
   static constexpr bool kFused = true;
 
   // FP32 copy of what the stages read: (r, r - r_plus), (p_r, p_theta) as packed pairs, theta
@@ -412,10 +423,14 @@ struct Mixed {
     Motion<float> mo;
   };
 
-  // The accepted state's diagnostics (Carter constant, axis test) use FP64 sine and cosine.
+  // The accepted state's sine and cosine: the mixed mode needs them only in FP32 (the shadow,
+  // the diagnostics), sincosf of theta rounded to float; the axis test works on theta itself.
   __device__ static Trig accept_trig(double th, const Trig&) {
+    float s, c;
+    sincosf((float)th, &s, &c);
     Trig t;
-    sincos(th, &t.s, &t.c);
+    t.s = (double)s;
+    t.c = (double)c;
     return t;
   }
 
@@ -459,6 +474,16 @@ struct Mixed {
     rhs_separated<float>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f);
   }
 };
+
+// The mixed mode with an infinite or NaN error norm taken as a rejection with the smallest step
+// factor (en^2 = inf or NaN: accept fails, the factor clamps to 1/5), which is what FP64 does
+// with the same trial step's huge but finite norm; a ray singular in FP64 as well keeps
+// shrinking its step below h_min and still ends as a NUMERICAL_FAILURE.  Used for the few rays
+// the mixed trace lost to an FP32 overflow (as the main kernel it costs about 5 % of its time:
+// code generation, the attempt counts being the same).
+struct MixedSat : Mixed {
+  static constexpr bool kSaturate = true;
+};
 // ------------------------------------------------------------------------------------------
 // The state of one ray between step attempts.
 // ------------------------------------------------------------------------------------------
@@ -491,6 +516,20 @@ __device__ __forceinline__ bool all_finite(const typename M::S y[NV], typename M
   return ok;
 }
 
+// |sin(theta)| < 1e-12 (classification.py:56): from the sine in the reference and fast64 modes;
+// in the mixed mode, whose sine is FP32, as min(|theta|, |pi - theta|) < 1e-12 in FP64 (sin x = x
+// to a relative 1e-24 there; theta lies in [-1e-9, pi + 1e-9] when this test runs).
+template <class M>
+__device__ __forceinline__ bool near_axis(const Ray<M>& ry) {
+  if constexpr (M::kMixed) {
+    const double th = ry.y[CTH];
+    return fmin(fabs(th), fabs(PI - th)) < AXIS_SIN_TOL;
+  } else {
+    using S = typename M::S;
+    return fabs((S)ry.tr.s) < (S)AXIS_SIN_TOL;
+  }
+}
+
 // Termination rules in the reference priority (numba_kernel.py:293-311).  Thresholds are
 // compared in the state type like the reference's working-dtype constants.
 // check_finite = false where the state and its right-hand side are already known finite (an
@@ -502,7 +541,7 @@ __device__ __forceinline__ int classify(const Params& P, const Ray<M>& ry, bool 
   if (check_h && ry.h < (S)P.h_min) return FAILURE;
   const S r = ry.y[CR], th = ry.y[CTH];
   if (r < (S)0.0 || th < (S)(-THETA_TOL) || th > (S)(PI + THETA_TOL)) return OUT_OF_DOMAIN;
-  if (ry.pph != (S)0.0 && fabs((S)ry.tr.s) < (S)AXIS_SIN_TOL) return OUT_OF_DOMAIN;
+  if (ry.pph != (S)0.0 && near_axis<M>(ry)) return OUT_OF_DOMAIN;
   if (r <= (S)P.r_capture) return CAPTURED;
   if (r >= (S)P.r_escape && ry.f[CR] > (typename M::K)0.0) return ESCAPED;
   if (ry.lam >= P.lambda_max || (long long)ry.n_steps >= P.max_steps) return MAX_AFFINE;
@@ -512,6 +551,14 @@ __device__ __forceinline__ int classify(const Params& P, const Ray<M>& ry, bool 
 // |(1/2) p_mu dx^mu/dlambda| in FP64, sequential order (numba_kernel.py:315-321).
 template <class M>
 __device__ __forceinline__ double null_error(const Ray<M>& ry) {
+  if constexpr (M::kMixed) {  // FP32, like the stages it checks
+    const Motion<float>& mo = ry.sh.mo;
+    float total = -mo.e * ry.f[CT];
+    total = fmaf(ry.sh.pp.x, ry.f[CR], total);
+    total = fmaf(ry.sh.pp.y, ry.f[CTH], total);
+    total = fmaf(mo.l, ry.f[CPH], total);
+    return (double)fabsf(0.5f * total);
+  }
   double total = (double)ry.pt * (double)ry.f[CT];
   total = total + (double)ry.y[CPR] * (double)ry.f[CR];
   total = total + (double)ry.y[CPTH] * (double)ry.f[CTH];
@@ -522,6 +569,12 @@ __device__ __forceinline__ double null_error(const Ray<M>& ry) {
 // Null Carter constant in FP64 (numba_kernel.py:325-336).
 template <class M>
 __device__ __forceinline__ double carter(const Params& P, const Ray<M>& ry) {
+  if constexpr (M::kMixed) {  // FP32 from the shadow, like the stages
+    const Mixed::Shadow& sh = ry.sh;
+    const float s = sh.s0, c = sh.c0, pth = sh.pp.y;
+    const float lz2_over_s2 = (sh.mo.l != 0.0f) ? (sh.mo.l * sh.mo.l) * rcp_fast(s * s) : 0.0f;
+    return (double)fmaf(pth, pth, (c * c) * (lz2_over_s2 - sh.mo.ae * sh.mo.ae));
+  }
   const double p_th = (double)ry.y[CPTH];
   const double lz = (double)ry.pph;
   const double e = -(double)ry.pt;
@@ -700,7 +753,8 @@ __device__ __forceinline__ void dp_stages_scalar(const Params& P, const Ray<M>& 
 __device__ __forceinline__ float2 mul2(float a, float2 x) { return __fmul2_rn(make_float2(a, a), x); }
 __device__ __forceinline__ float2 madd2(float2 acc, float a, float2 x) { return __ffma2_rn(make_float2(a, a), x, acc); }
 
-__device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<Mixed>& ry, float h, float k6[NV],
+template <class M>
+__device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<M>& ry, float h, float k6[NV],
                                                 double yn[NV], float esum[NV]) {
   auto c = [](double x) { return (float)x; };
   const Mixed::Shadow& sh = ry.sh;
@@ -768,9 +822,9 @@ template <class M, bool RK4>
 __device__ __forceinline__ void dp_stages(const Params& P, const Ray<M>& ry, typename M::K h, typename M::K k6[NV],
                                           typename M::S yn[NV], typename M::K esum[NV], Trig& tr,
                                           typename M::K (*acc_rec)[NV] = nullptr) {
-  if constexpr (std::is_same<M, Mixed>::value) {
+  if constexpr (M::kMixed) {
     static_assert(!RK4, "the mixed mode integrates with Dormand-Prince 5(4) only");
-    dp_stages_mixed(P, ry, h, k6, yn, esum);
+    dp_stages_mixed<M>(P, ry, h, k6, yn, esum);
   } else {
     dp_stages_scalar<M, RK4>(P, ry, h, k6, yn, esum, tr, acc_rec);
   }
@@ -827,7 +881,7 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
       // Full-state slots: 0 t, 1 r, 2 th, 3 ph, 4 p_t (0), 5 p_r, 6 p_th, 7 p_phi (0).
       const N total = ((q[CT] + q[CR]) + (q[CTH] + q[CPH])) + (q[CPR] + q[CPTH]);
       if constexpr (M::kFused) {
-        if (!finite_(total)) {
+        if (!M::kSaturate && !finite_(total)) {
           finite = false;
           accept = false;
         } else {

@@ -44,6 +44,13 @@ const Variant* fast_variants(bool mixed, bool rk4, int* count) {
   return f64;
 }
 
+// The mixed re-trace of the few rays an FP32 overflow ended early (MixedSat: an overflowing
+// trial step is a rejection, as in FP64).
+const Variant* mixed_sat_variant() {
+  static const Variant v = make_variant<MixedSat, false, 128, 4>();
+  return &v;
+}
+
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s) {
   return mixed ? run_bisect<Mixed, 128, 1>(a, s) : run_bisect<Fast64, 128, 3>(a, s);
 }

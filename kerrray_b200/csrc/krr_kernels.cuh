@@ -123,20 +123,46 @@ __global__ void k_trace_plain(Params P, const Image* __restrict__ images, int n_
 // risk (nullable, one byte per photon, from k_risk_prepass): RISK_CRITICAL photons are skipped
 // (retired unwritten: another kernel traces them), and a photon that ends within 1 % of its
 // affine or step budget is marked RISK_RECHECK (its class could depend on the last steps).
-// spread: a warp holds at most ceil(entries / warps) photons at a time, so a short queue is
-// shared by every warp of the grid instead of filling the first warps' lanes.
+// flags: TRACE_SPREAD -- a warp holds at most ceil(entries / warps) photons at a time, so a
+// short queue is shared by every warp of the grid instead of filling the first warps' lanes;
+// TRACE_RESUME -- a photon continues from the result row already in the outputs (its last
+// accepted state, affine parameter, counters and drift maxima: a trace that an FP32 overflow
+// ended early) with the first step size, instead of starting again at the camera.
+enum : int { TRACE_SPREAD = 1, TRACE_RESUME = 2 };
+
+template <class M>
+__device__ __forceinline__ void resume_from_outputs(const Params& P, const Outputs& o, long long g, Ray<M>& ry) {
+  using S = typename M::S;
+  using D = typename M::D;
+  if (!(o.lam && o.n_steps && o.n_rej)) return;  // nothing to resume from: start again
+  const double* Y = o.Y + g * 8;
+  ry.y[CT] = (S)Y[0];
+  ry.y[CR] = (S)Y[1];
+  ry.y[CTH] = (S)Y[2];
+  ry.y[CPH] = (S)Y[3];
+  ry.y[CPR] = (S)Y[5];
+  ry.y[CPTH] = (S)Y[6];
+  M::init_rhs(P, ry.y, ry.pt, ry.pph, ry.sh, ry.f, ry.tr);
+  ry.lam = o.lam[g];
+  ry.n_steps = (int)o.n_steps[g];
+  ry.n_rej = (int)o.n_rej[g];
+  if (o.max_null) ry.m_null = py_max(ry.m_null, (D)o.max_null[g]);
+  if (o.max_q) ry.m_q = (D)o.max_q[g];
+  ry.state = classify<M>(P, ry, false);
+}
+
 template <class M, bool RK4, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_trace_persistent(const Image* __restrict__ images, int n_images, long long total,
                        const double* __restrict__ Y0, Outputs o, Queue* __restrict__ q, int refill_threshold,
                        const long long* __restrict__ index, const unsigned long long* __restrict__ d_total,
-                       unsigned char* __restrict__ risk, int spread, int pdl) {
+                       unsigned char* __restrict__ risk, int flags, int pdl) {
   constexpr unsigned FULL = 0xffffffffu;
   if (pdl & PDL_TRIGGER) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if ((pdl & PDL_STAMP) && threadIdx.x == 0) atomicMin(&q->t_first, global_ns());
   if (d_total) total = (long long)*d_total;
   int cap = 32;
-  if (spread) {
+  if (flags & TRACE_SPREAD) {
     const long long warps = (long long)gridDim.x * (blockDim.x / 32);
     cap = (int)min(32LL, max(1LL, (total + warps - 1) / warps));
   }
@@ -190,6 +216,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
             double y0[8];
             photon_source(images, img, Y0, g, y0, q);
             ray_init<M>(im.P, y0, carter_initial(im.P, y0), ry);
+            if (flags & TRACE_RESUME) resume_from_outputs<M>(im.P, o, g, ry);
             if (ry.state == RUNNING) active = true;
             else retire();
           }
@@ -420,7 +447,7 @@ struct PersistArgs {
   const long long* index;             // re-trace list (nullable)
   const unsigned long long* d_total;  // device-side entry count (nullable)
   unsigned char* risk;                // analytic classes (nullable): skip the critical photons
-  int spread;                         // share a short queue over every warp
+  int flags;                          // TRACE_* bits
   int pdl;                            // PDL_* bits; with PDL_WAIT launched as a programmatic dependent
 };
 
@@ -446,7 +473,7 @@ cudaError_t run_persistent(const PersistArgs& a, cudaStream_t s) {
   cfg.attrs = attr;
   cfg.numAttrs = (a.pdl & PDL_WAIT) ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, k_trace_persistent<M, RK4, MAXT, MINB>, a.images, a.n_images, (long long)a.total,
-                            a.Y0, a.o, a.q, a.refill_threshold, a.index, a.d_total, a.risk, a.spread, a.pdl);
+                            a.Y0, a.o, a.q, a.refill_threshold, a.index, a.d_total, a.risk, a.flags, a.pdl);
 }
 
 template <class M, bool RK4, int MAXT, int MINB>

@@ -16,6 +16,7 @@ const Variant* ref_variants(bool dtype32, bool rk4, int* count);
 // Fast modes: mixed selects FP32 stages with FP64 accumulation; otherwise FP64.
 cudaError_t fast_plain(bool mixed, bool rk4, const PlainArgs& a, int block, cudaStream_t s);
 const Variant* fast_variants(bool mixed, bool rk4, int* count);
+const Variant* mixed_sat_variant();
 
 // Edge bisection launches (persistent, one item per lane).
 cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s);
