@@ -182,6 +182,15 @@ KRR_API int krr_integrate_batch_device(int device, double mass, double spin, con
                                const int64_t* d_index, int64_t n, const krr_options* options,
                                int32_t precision, const krr_result* d_out, void* stream);
 
+/* Where each escaped ray crosses r = r_surface: theta and phi of the rays whose state is ESCAPED
+ * (device arrays d_Y (n x 8), d_state (n)), flown back from the final state -- the first
+ * accepted state beyond the escape radius, which overshoots the surface by up to a step -- along
+ * the same Hamiltonian (FP64 RK4 substeps, Newton on the affine offset); NaN for the other rows.
+ * Two integrations of a ray are comparable there whatever steps they took.  Enqueued on
+ * `stream` without synchronising.  No counterpart in the reference. */
+KRR_API int krr_escape_directions(int device, double mass, double spin, double r_surface, const double* d_Y,
+                                  const int64_t* d_state, int64_t n, double* d_theta, double* d_phi, void* stream);
+
 /* Initial states of a pixel grid (alpha == beta == NULL: resolution^2 rows, row-major) or of n
  * arbitrary image points (alpha, beta host arrays of length n), written to host Y0 (rows x 8). */
 KRR_API int krr_camera_states(int device, double mass, double spin, const krr_camera* camera,

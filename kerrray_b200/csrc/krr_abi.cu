@@ -746,6 +746,30 @@ int krr_integrate_batch(int device, double mass, double spin, const double* Y0, 
   return KRR_OK;
 }
 
+int krr_escape_directions(int device, double mass, double spin, double r_surface, const double* d_Y,
+                          const int64_t* d_state, int64_t n, double* d_theta, double* d_phi, void* stream) {
+  int rc = validate_spacetime(mass, spin);
+  if (rc) return rc;
+  if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0");
+  if (!(r_surface > 0.0)) return fail(KRR_ERR_INVALID, "r_surface must be > 0, got %g", r_surface);
+  if (n == 0) return KRR_OK;
+  if (!d_Y || !d_state || !d_theta || !d_phi) return fail(KRR_ERR_INVALID, "device buffers must not be NULL");
+  krr_options o{};
+  o.rtol = 1e-6;
+  o.atol = 1e-8;
+  o.step_size = 0.01;
+  o.max_steps = 1;
+  o.lambda_max = 1.0;
+  o.h_min = 1e-12;
+  o.h_max = 1.0;
+  o.escape_radius = r_surface;
+  const krr::Params P = make_params(mass, spin, &o);
+  KRR_CUDA(cudaSetDevice(device));
+  KRR_CUDA(krr::escape_directions(P, r_surface, d_Y, reinterpret_cast<const long long*>(d_state), n, d_theta, d_phi,
+                                  static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
 int krr_camera_states(int device, double mass, double spin, const krr_camera* camera, const double* alpha,
                       const double* beta, int64_t n, double* Y0) {
   int rc = validate_spacetime(mass, spin);

@@ -1,6 +1,8 @@
 // Fast kernels: FP64 (Fast64) and FP32 stages with FP64 accumulation (Mixed).  Their FMAs are
 // written out in the source; the translation unit is compiled with -fmad=false so the compiler
 // fuses nothing else and every launch variant (register cap) computes identical results.
+#include <math_constants.h>
+
 #include "krr_launch.h"
 
 namespace krr {
@@ -49,6 +51,75 @@ const Variant* fast_variants(bool mixed, bool rk4, int* count) {
 const Variant* mixed_sat_variant() {
   static const Variant v = make_variant<MixedSat, false, 128, 4>();
   return &v;
+}
+
+// Where an escaped ray crosses r = r_s: from its final state (the first accepted state at or
+// beyond the escape radius, which overshoots the surface by up to a step), flow back along the
+// same Hamiltonian in FP64 (classical RK4, 32 substeps of the FP64 separated right-hand side)
+// over the affine offset dl that Newton's method drives to r(dl) = r_s (dr/dl = f_r), three
+// iterations from the linear estimate.  Gives theta and phi on the surface, the quantities two
+// integrations of the same ray can be compared on whatever steps they took.
+__device__ void flow_rk4(const Params& P, double y[8], double dl, int n) {
+  const double hh = dl / n;
+  auto f8 = [&](const double z[8], double out[8]) {
+    double f[NV];
+    Trig tr;
+    Fast64::rhs(P, z[1], z[2], z[4], z[5], z[6], z[7], f, tr);
+    out[0] = f[CT];
+    out[1] = f[CR];
+    out[2] = f[CTH];
+    out[3] = f[CPH];
+    out[4] = 0.0;
+    out[5] = f[CPR];
+    out[6] = f[CPTH];
+    out[7] = 0.0;
+  };
+  for (int k = 0; k < n; ++k) {
+    double k1[8], k2[8], k3[8], k4[8], z[8];
+    f8(y, k1);
+    for (int i = 0; i < 8; ++i) z[i] = fma(0.5 * hh, k1[i], y[i]);
+    f8(z, k2);
+    for (int i = 0; i < 8; ++i) z[i] = fma(0.5 * hh, k2[i], y[i]);
+    f8(z, k3);
+    for (int i = 0; i < 8; ++i) z[i] = fma(hh, k3[i], y[i]);
+    f8(z, k4);
+    for (int i = 0; i < 8; ++i) y[i] = fma(hh / 6.0, k1[i] + 2.0 * (k2[i] + k3[i]) + k4[i], y[i]);
+  }
+}
+
+__global__ void k_escape_directions(Params P, double r_s, const double* __restrict__ Y,
+                                    const long long* __restrict__ state, long long n, double* __restrict__ theta,
+                                    double* __restrict__ phi) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double th = CUDART_NAN, ph = CUDART_NAN;
+  if (state[i] == ESCAPED) {
+    double y0[8], y[8], f[NV];
+    Trig tr;
+    for (int c = 0; c < 8; ++c) y0[c] = Y[i * 8 + c];
+    Fast64::rhs(P, y0[1], y0[2], y0[4], y0[5], y0[6], y0[7], f, tr);
+    double dl = -(y0[1] - r_s) / f[CR];
+    for (int it = 0; it < 3; ++it) {
+      for (int c = 0; c < 8; ++c) y[c] = y0[c];
+      flow_rk4(P, y, dl, 32);
+      Fast64::rhs(P, y[1], y[2], y[4], y[5], y[6], y[7], f, tr);
+      dl -= (y[1] - r_s) / f[CR];
+    }
+    for (int c = 0; c < 8; ++c) y[c] = y0[c];
+    flow_rk4(P, y, dl, 32);
+    th = y[2];
+    ph = y[3];
+  }
+  theta[i] = th;
+  phi[i] = ph;
+}
+
+cudaError_t escape_directions(const Params& P, double r_s, const double* Y, const long long* state, long long n,
+                              double* theta, double* phi, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int block = 128;
+  k_escape_directions<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(P, r_s, Y, state, n, theta, phi);
+  return cudaGetLastError();
 }
 
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s) {

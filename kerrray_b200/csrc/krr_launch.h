@@ -18,6 +18,11 @@ cudaError_t fast_plain(bool mixed, bool rk4, const PlainArgs& a, int block, cuda
 const Variant* fast_variants(bool mixed, bool rk4, int* count);
 const Variant* mixed_sat_variant();
 
+// theta and phi where each escaped ray (state ESCAPED) crosses r = r_s, flown back from its final
+// state Y; NaN for the other rows.
+cudaError_t escape_directions(const Params& P, double r_s, const double* Y, const long long* state, long long n,
+                              double* theta, double* phi, cudaStream_t s);
+
 // Edge bisection launches (persistent, one item per lane).
 cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s);
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s);

@@ -27,10 +27,29 @@ from kerrray_b200.camera import Camera
 from kerrray_b200.types import BatchResult, TerminationState
 
 __all__ = ["ImageSpec", "SweepResult", "DeviceSweep", "LaunchConfig", "order_by_cost", "trace_images", "RETRACE_EDGE",
-           "RETRACE_CRITICAL", "analytic_classes"]
+           "RETRACE_CRITICAL", "analytic_classes", "escape_directions"]
 
 RETRACE_EDGE = 1
 RETRACE_CRITICAL = 2
+
+
+def escape_directions(spacetime, Y, state, r_surface: float):
+    """(theta, phi) where each escaped ray crosses r = r_surface (``krr_escape_directions``), for
+    device tensors ``Y`` (n x 8, float64) and ``state`` (n, int64); NaN where not ESCAPED. Two
+    integrations of the same rays are comparable there whatever steps they took."""
+    import torch
+
+    if Y.device.type != "cuda" or Y.dtype != torch.float64 or state.dtype != torch.int64:
+        raise ValueError("Y must be a float64 and state an int64 CUDA tensor")
+    n = int(state.numel())
+    Y, state = Y.contiguous(), state.contiguous()
+    theta = torch.empty(n, dtype=torch.float64, device=Y.device)
+    phi = torch.empty(n, dtype=torch.float64, device=Y.device)
+    stream = torch.cuda.current_stream(Y.device).cuda_stream
+    _lib.check(_lib.lib().krr_escape_directions(Y.device.index, float(spacetime.mass), float(spacetime.spin),
+                                                float(r_surface), Y.data_ptr(), state.data_ptr(), n,
+                                                theta.data_ptr(), phi.data_ptr(), stream))
+    return theta, phi
 
 
 def analytic_classes(spacetime, y0: np.ndarray, rtol: float, horizon_epsilon: float = 1e-6) -> np.ndarray:

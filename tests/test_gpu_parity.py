@@ -490,6 +490,33 @@ def _land(O, spin: float, y: np.ndarray, rs: float) -> np.ndarray:
     return flow(y, dl)
 
 
+def test_escape_directions_land_on_the_surface() -> None:
+    """theta, phi where the reference's escaped rays (64^2 golden image) cross r = 1000: the
+    device landing against the oracle's host landing (RK4 on the reference's right-hand side)."""
+    torch = pytest.importorskip("torch")
+    from oracle import oracle as O
+
+    d = golden("shadow64_a0.9_i60")
+    state = d["state"].astype(np.int64)
+    Y = torch.tensor(d["Y"], dtype=torch.float64, device="cuda")
+    th, ph = K.escape_directions(K.Spacetime(1.0, 0.9), Y, torch.tensor(state, device="cuda"), 1000.0)
+    th, ph = th.cpu().numpy(), ph.cpu().numpy()
+    assert np.all(np.isnan(th[state != 1])) and np.all(np.isfinite(th[state == 1]))
+    esc = np.flatnonzero(state == 1)[::180][:16]
+    ref = np.array([_land(O, 0.9, d["Y"][i], 1000.0)[2:4] for i in esc])
+    err = np.abs(np.stack([th[esc], ph[esc]], axis=1) - ref).max()
+    print("escape directions vs oracle landing: max", err)
+    assert err < 1e-9
+    # The same rays integrated by fast64 (another step sequence) land within the tolerance's reach.
+    res = K.CudaBackend(precision="fast64").integrate_batch(K.Spacetime(1.0, 0.9), d["Y0"], K.IntegratorOptions(rtol=1e-6, atol=1e-8),
+                                                            K.TerminationOptions())
+    th2, ph2 = K.escape_directions(K.Spacetime(1.0, 0.9), torch.tensor(res.Y, device="cuda"),
+                                   torch.tensor(res.state.astype(np.int64), device="cuda"), 1000.0)
+    both = (state == 1) & (res.state == 1)
+    dth = np.abs(th2.cpu().numpy()[both] - th[both])
+    assert np.median(dth) < 1e-5, np.median(dth)
+
+
 def test_adjoint_against_finite_differences_of_the_reference() -> None:
     """Adjoint Jacobian vs central FD (h = 1e-6) of the oracle (the reference's Numba kernel
     restated, adaptive controller live) at the same rtol 1e-10, each oracle trajectory taken to
