@@ -317,6 +317,15 @@ KRR_API int krr_trace_images_noalloc(int device, const krr_image* images, int32_
  * dependent FMA chains timed with CUDA events; the roofline denominator of the step kernels. */
 KRR_API int krr_fma_peak(int device, int fp64, double* tflops);
 
+/* Accuracy utility with no counterpart in the reference: the step kernels' own sine and cosine
+ * forms at n angles (device arrays), enqueued on `stream`.  which 0: the FP32 sine and cosine of
+ * an FP64 angle (reduced by the nearest multiple of pi/2; the mixed mode's accepted states);
+ * 1: the FP32 small-angle shift from the FP32-rounded sine and cosine of theta by (float)delta
+ * (the mixed stages); 2: the FP64 shift by delta (the fast64 stages).  Results as FP64; NaN where
+ * a shift declines (|delta| above 1/4 in FP32, 1/10 in FP64).  d_delta may be NULL for which 0. */
+KRR_API int krr_trig_eval(int device, int32_t which, const double* d_theta, const double* d_delta, int64_t n,
+                          double* d_sin, double* d_cos, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

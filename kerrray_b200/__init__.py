@@ -46,6 +46,7 @@ from kerrray_b200.sweep import (
     SweepResult,
     analytic_classes,
     escape_directions,
+    trig_eval,
     order_by_cost,
     trace_images,
 )
@@ -81,5 +82,5 @@ __all__ = [
     "SweepResult", "TerminationOptions", "TerminationState", "autotune", "available_backends", "compute_shadow",
     "concatenate_results", "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
     "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
-    "RETRACE_CRITICAL", "RETRACE_EDGE", "analytic_classes", "escape_directions",
+    "RETRACE_CRITICAL", "RETRACE_EDGE", "analytic_classes", "escape_directions", "trig_eval",
 ]

@@ -746,6 +746,18 @@ int krr_integrate_batch(int device, double mass, double spin, const double* Y0, 
   return KRR_OK;
 }
 
+int krr_trig_eval(int device, int32_t which, const double* d_theta, const double* d_delta, int64_t n, double* d_sin,
+                  double* d_cos, void* stream) {
+  if (which < 0 || which > 2) return fail(KRR_ERR_INVALID, "which must be 0, 1 or 2, got %d", which);
+  if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0");
+  if (n == 0) return KRR_OK;
+  if (!d_theta || !d_sin || !d_cos || (which != 0 && !d_delta))
+    return fail(KRR_ERR_INVALID, "device buffers must not be NULL (d_delta may be NULL only for which 0)");
+  KRR_CUDA(cudaSetDevice(device));
+  KRR_CUDA(krr::trig_eval(which, d_theta, d_delta, n, d_sin, d_cos, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
 int krr_escape_directions(int device, double mass, double spin, double r_surface, const double* d_Y,
                           const int64_t* d_state, int64_t n, double* d_theta, double* d_phi, void* stream) {
   int rc = validate_spacetime(mass, spin);

@@ -347,6 +347,36 @@ __device__ __forceinline__ bool sincos_shift_x2(float s0, float c0, float d, flo
   return true;
 }
 
+// sin and cos of an FP64 angle to FP32 accuracy (the mixed mode's accepted states and its rare
+// stage fallback), in about twenty instructions and no slow path:
+// - Cody and Waite's reduction by the nearest multiple k of pi/2, in FP64 with pi/2 split in two
+//   (x = th - k pi/2, |x| <= pi/4, for |th| < 2^51).  Next to the axis (th near 0 or pi) x keeps
+//   its relative accuracy.  k is rounded to nearest by adding 1.5 * 2^52, whose low word is then
+//   k mod 2^32;
+// - the Taylor series of sin(x)/x through x^8 and of cos x through x^10, in x^2, on packed pairs
+//   (truncation below 3e-9 and 1.2e-10 of the value for |x| <= pi/4);
+// - k mod 4 picks the pair and its signs.
+__device__ __forceinline__ void sincos_reduced(double th, float& s, float& c) {
+  constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  constexpr double kPio2Hi = 1.5707963267948966, kPio2Lo = 6.123233995736766e-17;
+  const double t = fma(th, 2.0 / PI, kRound);
+  const int q = __double2loint(t);
+  const double k = t - kRound;
+  const float x = (float)fma(-k, kPio2Lo, fma(-k, kPio2Hi, th));
+  const float x2 = x * x;
+  const float2 dd = f2(x2, x2);
+  float2 p = __ffma2_rn(dd, f2(0.0f, -1.0f / 3628800.0f), f2(1.0f / 362880.0f, 1.0f / 40320.0f));
+  p = __ffma2_rn(dd, p, f2(-1.0f / 5040.0f, -1.0f / 720.0f));
+  p = __ffma2_rn(dd, p, f2(1.0f / 120.0f, 1.0f / 24.0f));
+  p = __ffma2_rn(dd, p, f2(-1.0f / 6.0f, -0.5f));
+  p = __ffma2_rn(dd, p, f2(1.0f, 1.0f));  // (sin x / x, cos x)
+  const float sx = x * p.x, cx = p.y;
+  const float u = (q & 1) ? cx : sx;
+  const float v = (q & 1) ? sx : cx;
+  s = (q & 2) ? -u : u;
+  c = ((q + 1) & 2) ? -v : v;
+}
+
 // FP64 with explicit FMAs, sincos and Newton reciprocals on the separated form.
 struct Fast64 {
   using S = double;
@@ -432,10 +462,10 @@ struct Mixed {
   };
 
   // The accepted state's sine and cosine: the mixed mode needs them only in FP32 (the shadow,
-  // the diagnostics), sincosf of theta rounded to float; the axis test works on theta itself.
+  // the diagnostics), from theta in FP64 (sincos_reduced); the axis test works on theta itself.
   __device__ static Trig accept_trig(double th, const Trig&) {
     float s, c;
-    sincosf((float)th, &s, &c);
+    sincos_reduced(th, s, c);
     Trig t;
     t.s = (double)s;
     t.c = (double)c;
@@ -461,14 +491,15 @@ struct Mixed {
   // The right-hand side at the stage input shadow + h * acc, from the pairs (r, theta) and
   // (p_r, p_theta) of acc; k receives f as the pairs (r, theta), (p_r, p_theta), (t, phi).
   // Every stage's sine and cosine come from the accepted state's by a small-angle shift; near
-  // the axis (|sin| < 1/50, where the shift's sum would cancel) or for a large shift, sincosf.
+  // the axis (|sin| < 1/50, where the shift's sum would cancel) or for a large shift,
+  // sincos_reduced of the stage's theta.
   __device__ static void stage(const Params& P, const Shadow& sh, float h, const float2 acc[2], float2 k[3]) {
     const float2 hh = make_float2(h, h);
     const float2 rd = __ffma2_rn(hh, make_float2(acc[0].x, acc[0].x), sh.rd);  // (r, r - r_plus)
     const float2 pp = __ffma2_rn(hh, acc[1], sh.pp);                           // (p_r, p_theta)
     const float dth = h * acc[0].y;
     float s, c;
-    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift_x2(sh.s0, sh.c0, dth, s, c))) sincosf(sh.th + dth, &s, &c);
+    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift_x2(sh.s0, sh.c0, dth, s, c))) sincos_reduced((double)(sh.th + dth), s, c);
     float f[NV];
     rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, f);
     k[0] = make_float2(f[CR], f[CTH]);

@@ -122,6 +122,50 @@ cudaError_t escape_directions(const Params& P, double r_s, const double* Y, cons
   return cudaGetLastError();
 }
 
+// The step kernels' own sines and cosines at given angles, for accuracy checks: which 0 is
+// sincos_reduced(theta) (FP32, the mixed mode's accepted states); 1 is sincos_shift_x2 from the
+// FP32-rounded sine and cosine of theta by (float)delta (the mixed stages); 2 is sincos_shift from
+// the FP64 sine and cosine of theta by delta (the fast64 stages).  NaN where a shift declines.
+__global__ void k_trig_eval(int which, const double* __restrict__ theta, const double* __restrict__ delta, long long n,
+                            double* __restrict__ s_out, double* __restrict__ c_out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double th = theta[i];
+  double s = CUDART_NAN, c = CUDART_NAN;
+  if (which == 0) {
+    float fs, fc;
+    sincos_reduced(th, fs, fc);
+    s = fs;
+    c = fc;
+  } else {
+    double s0, c0;
+    sincos(th, &s0, &c0);
+    if (which == 1) {
+      float fs, fc;
+      if (sincos_shift_x2((float)s0, (float)c0, (float)delta[i], fs, fc)) {
+        s = fs;
+        c = fc;
+      }
+    } else {
+      double ds, dc;
+      if (sincos_shift(s0, c0, delta[i], ds, dc)) {
+        s = ds;
+        c = dc;
+      }
+    }
+  }
+  s_out[i] = s;
+  c_out[i] = c;
+}
+
+cudaError_t trig_eval(int which, const double* theta, const double* delta, long long n, double* s_out, double* c_out,
+                      cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int block = 256;
+  k_trig_eval<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(which, theta, delta, n, s_out, c_out);
+  return cudaGetLastError();
+}
+
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s) {
   return mixed ? run_bisect<Mixed, 128, 1>(a, s) : run_bisect<Fast64, 128, 3>(a, s);
 }

@@ -23,6 +23,11 @@ const Variant* mixed_sat_variant();
 cudaError_t escape_directions(const Params& P, double r_s, const double* Y, const long long* state, long long n,
                               double* theta, double* phi, cudaStream_t s);
 
+// The step kernels' sine and cosine forms at given angles (which: 0 FP32 reduced, 1 FP32 shift,
+// 2 FP64 shift; see k_trig_eval).
+cudaError_t trig_eval(int which, const double* theta, const double* delta, long long n, double* s_out, double* c_out,
+                      cudaStream_t s);
+
 // Edge bisection launches (persistent, one item per lane).
 cudaError_t ref_bisect(const EdgeArgs& a, cudaStream_t s);
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s);

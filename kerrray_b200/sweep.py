@@ -27,7 +27,7 @@ from kerrray_b200.camera import Camera
 from kerrray_b200.types import BatchResult, TerminationState
 
 __all__ = ["ImageSpec", "SweepResult", "DeviceSweep", "LaunchConfig", "order_by_cost", "trace_images", "RETRACE_EDGE",
-           "RETRACE_CRITICAL", "analytic_classes", "escape_directions"]
+           "RETRACE_CRITICAL", "analytic_classes", "escape_directions", "trig_eval"]
 
 RETRACE_EDGE = 1
 RETRACE_CRITICAL = 2
@@ -50,6 +50,30 @@ def escape_directions(spacetime, Y, state, r_surface: float):
                                                 float(r_surface), Y.data_ptr(), state.data_ptr(), n,
                                                 theta.data_ptr(), phi.data_ptr(), stream))
     return theta, phi
+
+
+def trig_eval(which: int, theta, delta=None):
+    """The step kernels' sine and cosine forms at the angles of the float64 CUDA tensor ``theta``
+    (``krr_trig_eval``): 0 the FP32 sine/cosine of an FP64 angle (mixed accepted states), 1 the
+    FP32 shift by ``delta`` from theta's FP32-rounded sine/cosine (mixed stages), 2 the FP64 shift
+    by ``delta`` (fast64 stages). Returns (sin, cos) as float64 tensors, NaN where a shift declines."""
+    import torch
+
+    if theta.device.type != "cuda" or theta.dtype != torch.float64:
+        raise ValueError("theta must be a float64 CUDA tensor")
+    theta = theta.contiguous()
+    if delta is not None:
+        if delta.device != theta.device or delta.dtype != torch.float64 or delta.numel() != theta.numel():
+            raise ValueError("delta must be a float64 tensor on theta's device, with theta's length")
+        delta = delta.contiguous()
+    n = int(theta.numel())
+    s = torch.empty(n, dtype=torch.float64, device=theta.device)
+    c = torch.empty(n, dtype=torch.float64, device=theta.device)
+    stream = torch.cuda.current_stream(theta.device).cuda_stream
+    _lib.check(_lib.lib().krr_trig_eval(theta.device.index, int(which), theta.data_ptr(),
+                                        None if delta is None else delta.data_ptr(), n, s.data_ptr(),
+                                        c.data_ptr(), stream))
+    return s, c
 
 
 def analytic_classes(spacetime, y0: np.ndarray, rtol: float, horizon_epsilon: float = 1e-6) -> np.ndarray:
