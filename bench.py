@@ -597,7 +597,8 @@ def run_bisect(args) -> None:
     line = _line("edge-bisection rays/s per B200 (batched, one persistent launch)", rays / (kernel_ms * 1e-3),
                  "rays/s", args, kernel_ms,
                  {"workload": WORKLOADS["bisect"], "items": n_items, "iterations": iterations, "cases": len(cases),
-                  "precision": precision, "kernel": "k_bisect_edges (one item per lane, all halvings in registers)",
+                  "precision": precision, "kernel": "k_bisect_edges (one item per lane, all halvings in registers; idle lanes trace the "
+                            "next midpoints ahead, results bit-identical to sequential bisection)",
                   "l2": "inputs < 1 MB; the work is FP64 arithmetic in registers"},
                  e2e={"value": rays / statistics.mean(walls), "unit": "rays/s", "h2d_bytes_per_step": n_items * 36,
                       "d2h_bytes_per_step": n_items * 24},
@@ -608,7 +609,11 @@ def run_bisect(args) -> None:
                  cpu_baseline=cpu, clocks=clocks.summary(), edge_error_vs_bardeen=summary,
                  worst_cases=sorted(per_case, key=lambda d: -d["max_M"])[:6],
                  queue={"attempts": stats["attempts"], "accepted": stats["accepted"],
-                        "lane_occupancy": stats["busy_slots"] / max(stats["lane_slots"], 1)})
+                        "lane_occupancy": stats["busy_slots"] / max(stats["lane_slots"], 1),
+                        "speculative_photons": stats["speculative"],
+                        "discarded_attempts": stats["discarded_attempts"],
+                        "note": "attempts: the sequential bisection's; discarded attempts (midpoints traced "
+                                "ahead on the side not taken) are outside the roofline's work"})
     print(json.dumps(line), flush=True)
 
 

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define KRR_ABI_VERSION 2
+#define KRR_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define KRR_API __attribute__((visibility("default")))
@@ -162,6 +162,9 @@ typedef struct krr_stats {
   uint64_t critical;    /* KRR_RETRACE_CRITICAL: photons in the critical band (traced beside) */
   uint64_t rechecked;   /* KRR_RETRACE_CRITICAL: photons traced again after the check */
   double critical_ms;   /* KRR_RETRACE_CRITICAL: device time of the critical-set kernel */
+  uint64_t speculative; /* krr_bisect_edges: photons traced ahead of their bracket by idle lanes */
+  uint64_t discarded_attempts; /* krr_bisect_edges: attempts of those photons whose side was not
+                                  taken (not in `attempts`, which counts the sequential bisection's) */
 } krr_stats;
 
 KRR_API const char* krr_last_error(void);

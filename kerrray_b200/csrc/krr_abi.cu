@@ -381,7 +381,8 @@ struct WorkLayout {
 };
 
 constexpr size_t round256(size_t x) { return (x + 255) / 256 * 256; }
-constexpr size_t kQueueArea = 1024;
+constexpr size_t kQueueArea = 1024;  // four queues, 256 bytes apart
+static_assert(sizeof(krr::Queue) <= 256, "a queue must fit its 256-byte slot of the workspace");
 
 size_t work_bytes(int n_images, long long list_entries) {
   const size_t n = (size_t)std::max(list_entries, 0LL);
@@ -1075,8 +1076,29 @@ int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, co
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(ctx->mu);
   KRR_CUDA(cudaSetDevice(device));
+  // Queue order: the cases' items dealt round robin, so that every warp holds items of every
+  // tolerance, and the cheap ones, ending early, lend their lanes to the expensive ones.  That
+  // needs the cases' parameters in shared memory (krr::edge_params_in_smem); with more cases
+  // the items keep their order, and a warp's lanes mostly share a case.
+  const bool interleave = krr::edge_params_in_smem(n_cases);
+  std::vector<long long> order((size_t)n_items);
+  for (int64_t i = 0; i < n_items; ++i) order[(size_t)i] = i;
+  if (interleave) {
+    std::vector<long long> start((size_t)n_cases + 1, 0), fill((size_t)n_cases, 0);
+    for (int64_t i = 0; i < n_items; ++i) start[(size_t)item_case[i] + 1] += 1;
+    for (int k = 0; k < n_cases; ++k) start[(size_t)k + 1] += start[(size_t)k];
+    std::vector<long long> by_case((size_t)n_items);
+    for (int64_t i = 0; i < n_items; ++i) {
+      const int k = item_case[i];
+      by_case[(size_t)(start[(size_t)k] + fill[(size_t)k]++)] = i;
+    }
+    size_t n = 0;
+    for (long long r = 0; n < (size_t)n_items; ++r)
+      for (int k = 0; k < n_cases; ++k)
+        if (start[(size_t)k] + r < start[(size_t)k + 1]) order[n++] = by_case[(size_t)(start[(size_t)k] + r)];
+  }
   const size_t nb8 = (size_t)n_items * 8, nb4 = (size_t)n_items * 4;
-  const size_t bytes = 512 + round256((size_t)n_cases * sizeof(krr::EdgeCase)) + 5 * round256(nb8) + round256(nb4);
+  const size_t bytes = 512 + round256((size_t)n_cases * sizeof(krr::EdgeCase)) + 6 * round256(nb8) + round256(nb4);
   KRR_CUDA(ctx->buf[B_AB].ensure(bytes));
   char* base = static_cast<char*>(ctx->buf[B_AB].p);
   krr::Queue* d_q = reinterpret_cast<krr::Queue*>(base);
@@ -1089,6 +1111,7 @@ int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, co
   auto* d_lo = reinterpret_cast<double*>(take(nb8));
   auto* d_hi = reinterpret_cast<double*>(take(nb8));
   auto* d_fail = reinterpret_cast<long long*>(take(nb8));
+  auto* d_order = reinterpret_cast<long long*>(take(nb8));
   const cudaStream_t s = ctx->stream;
   KRR_CUDA(cudaMemsetAsync(d_q, 0, sizeof(krr::Queue), s));
   KRR_CUDA(cudaMemcpyAsync(d_cases, ec.data(), ec.size() * sizeof(krr::EdgeCase), cudaMemcpyHostToDevice, s));
@@ -1097,6 +1120,7 @@ int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, co
   KRR_CUDA(cudaMemcpyAsync(d_sin, sin_phi, nb8, cudaMemcpyHostToDevice, s));
   KRR_CUDA(cudaMemcpyAsync(d_lo, lo, nb8, cudaMemcpyHostToDevice, s));
   KRR_CUDA(cudaMemcpyAsync(d_hi, hi, nb8, cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemcpyAsync(d_order, order.data(), nb8, cudaMemcpyHostToDevice, s));
   krr::EdgeArgs a{};
   a.cases = d_cases;
   a.item_case = d_item;
@@ -1105,6 +1129,8 @@ int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, co
   a.lo = d_lo;
   a.hi = d_hi;
   a.failures = d_fail;
+  a.order = d_order;
+  a.n_cases = n_cases;
   a.n_items = n_items;
   a.iterations = iterations;
   a.q = d_q;
@@ -1124,11 +1150,13 @@ int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_cases, co
     std::memset(stats, 0, sizeof(*stats));
     stats->photons = (uint64_t)n_items * (uint64_t)iterations;
     stats->retired = q.retired;
-    stats->attempts = q.attempts;
+    stats->attempts = q.attempts - q.discarded;  // the sequential bisection's attempts
     stats->accepted = q.accepted;
     stats->lane_slots = q.lane_iters;
-    stats->busy_slots = q.busy_iters;
+    stats->busy_slots = q.busy_iters;             // every attempt run, discarded ones included
     stats->kernel_ms = ms;
+    stats->speculative = q.speculative;
+    stats->discarded_attempts = q.discarded;
   }
   if (q.error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
   if (q.retired != (unsigned long long)n_items)

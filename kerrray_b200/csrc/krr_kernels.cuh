@@ -39,6 +39,8 @@ struct Queue {
   unsigned long long flagged;     // photons appended to the re-trace list
   unsigned long long t_first;     // globaltimer (ns) of the first block's start (PDL_STAMP), from ~0
   unsigned long long t_last;      // globaltimer (ns) of the last block's end (PDL_STAMP)
+  unsigned long long speculative; // edge bisection: photons traced ahead of their bracket
+  unsigned long long discarded;   // edge bisection: attempts of speculative photons not needed
 };
 
 // Programmatic dependent launch (sm_90+) of the persistent kernel, as bits of its `pdl`
@@ -280,8 +282,21 @@ __global__ void __launch_bounds__(MAXT, MINB)
 // image radius rho is bisected between a bracket [lo, hi] (captured at lo, escaped at hi): a
 // photon at alpha = c_a + mid cos(phi), beta = c_b + mid sin(phi), mid = (lo + hi) / 2, is
 // traced; ESCAPED moves hi to mid, anything else moves lo to mid; a result that is neither
-// ESCAPED nor CAPTURED counts as a failure.  One lane owns one item and runs all its
-// iterations; lanes refill from the queue when their item is done.
+// ESCAPED nor CAPTURED counts as a failure.
+//
+// One lane owns an item and runs its halvings one after another.  Once the queue is drained,
+// a warp's idle lanes trace ahead: a helper takes a node of the bisection tree below an
+// owner's current bracket, at depth 1..KRR_EDGE_DEPTH (the brackets the item holds after the
+// owner's photon and the next ones, for either outcome), and traces its midpoint while the
+// owner's photon is still running.  When the owner's photon ends, the helpers on the outcome's
+// side move up one level; the one at depth 1 inherits the item and continues with its photon
+// (possibly already ended, which settles one more halving at once); the helpers on the other
+// side are discarded.  Every midpoint is 0.5 * (lo + hi) of the bracket the sequential
+// bisection would hold there, so the results are the sequential ones bit for bit.  Lanes are
+// given to the shallowest untraced nodes first, across the warp's owners.  A warp's lanes
+// share its instructions, so a helper costs issue slots only where its warp would otherwise
+// have ended; the host interleaves the items of all cases so that every warp holds cheap items,
+// which end early and lend their lanes, beside expensive ones.
 // ------------------------------------------------------------------------------------------
 struct EdgeCase {
   Params P;
@@ -297,6 +312,8 @@ struct EdgeArgs {
   double* lo;
   double* hi;
   long long* failures;
+  const long long* order;  // queue position -> item (nullable: identity)
+  int n_cases;
   long long n_items;
   int iterations;
   Queue* q;
@@ -323,50 +340,142 @@ __device__ __forceinline__ void edge_start(const EdgeArgs& a, EdgeLane<M>& L) {
   ray_init<M>(ec.P, y0, carter_initial(ec.P, y0), L.ry);
 }
 
-// The photon of the current iteration has terminated: update the bracket; start the next
-// iteration, or return false when the item is done.
-template <class M>
-__device__ __forceinline__ bool edge_next(const EdgeArgs& a, EdgeLane<M>& L) {
-  const int st = L.ry.state;
-  if (st != ESCAPED && st != CAPTURED) L.fails += 1;
-  if (st == ESCAPED) L.hi = L.mid; else L.lo = L.mid;
-  L.it += 1;
-  if (L.it >= a.iterations) return false;
-  edge_start<M>(a, L);
-  return true;
+enum : int { EDGE_IDLE = 0, EDGE_OWNER = 1, EDGE_HELPER = 2 };
+
+#ifndef KRR_EDGE_DEPTH
+#define KRR_EDGE_DEPTH 4
+#endif
+// Nodes below an owner's bracket, depth d = 1..KRR_EDGE_DEPTH, path p (d bits, the first step
+// in the highest bit; 1 = the photon before escaped): bit (2^d - 2 + p) of a 32-bit mask.
+constexpr int EDGE_DEPTH = KRR_EDGE_DEPTH;
+static_assert(EDGE_DEPTH >= 1 && EDGE_DEPTH <= 4, "the node masks hold depths 1..4");
+__device__ __forceinline__ int edge_node(int d, int p) { return (1 << d) - 2 + p; }
+
+__device__ __forceinline__ int nth_set_bit(unsigned mask, int n) {
+  for (int i = 0; i < n; ++i) mask &= mask - 1u;
+  return __ffs(mask) - 1;
 }
 
-template <class M, int MAXT, int MINB>
+// The cases' step parameters are staged in shared memory when they fit: a warp's lanes hold
+// items of different cases, and each parameter load is then one shared-memory access (the
+// 184-byte stride, 23 doubles, is odd: no bank conflicts) instead of one global-memory
+// wavefront per distinct case.
+constexpr size_t kEdgeSmemMax = 48 * 1024;
+__host__ __device__ constexpr bool edge_params_in_smem(int n_cases) {
+  return (size_t)n_cases * sizeof(Params) <= kEdgeSmemMax;
+}
+
+template <class M, int MAXT, int MINB, bool SMEM>
 __global__ void __launch_bounds__(MAXT, MINB) k_bisect_edges(EdgeArgs a) {
   constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char edge_smem[];
+  Params* s_params = reinterpret_cast<Params*>(edge_smem);
+  if constexpr (SMEM) {
+    static_assert(sizeof(Params) % 8 == 0, "Params is copied in 8-byte words");
+    constexpr int words = (int)(sizeof(Params) / 8);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(s_params);
+    for (int k = threadIdx.x; k < a.n_cases * words; k += blockDim.x)
+      dst[k] = reinterpret_cast<const unsigned long long*>(&a.cases[k / words].P)[k % words];
+    __syncthreads();
+  }
+  auto params = [&](int c) -> const Params& {
+    if constexpr (SMEM) return s_params[c];
+    else return a.cases[c].P;
+  };
+  __shared__ int slots[MAXT];  // 32 per warp, indexed by lane
+  int* slot = slots + (threadIdx.x & ~31u);
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   EdgeLane<M> L;
   L.ry.state = FAILURE;
-  bool active = false, drained = false;
+  L.lo = L.hi = L.mid = L.cphi = L.sphi = 0.0;
+  L.fails = 0;
+  L.it = L.c = 0;
+  int role = EDGE_IDLE, host = 0, depth = 0, path = 0;
+  bool drained = false, dirty = true;
   long long g = -1;
-  unsigned long long my_attempts = 0, my_accepted = 0;  // every busy lane slot is one attempt
+  unsigned long long my_attempts = 0, my_accepted = 0, my_spec = 0, my_discarded = 0;
   unsigned my_iters = 0;
   auto finish_item = [&]() {
     a.lo[g] = L.lo;
     a.hi[g] = L.hi;
     if (a.failures) a.failures[g] = L.fails;
     atomicAdd(&a.q->retired, 1ull);
-    active = false;
+    role = EDGE_IDLE;
+  };
+  // Settle every owner whose photon has ended, repeatedly: an heir whose photon had ended too
+  // settles the next halving in the following pass.
+  auto resolve = [&]() {
+    while (true) {
+      const bool ended = role == EDGE_OWNER && L.ry.state != RUNNING;
+      const unsigned em = __ballot_sync(FULL, ended);
+      if (em == 0) break;
+      dirty = true;
+      int want = -1;  // the side the item continues on: 1 escaped, 0 otherwise; -1 item done
+      if (ended) {
+        my_accepted += (unsigned long long)L.ry.n_steps;
+        const int st = L.ry.state;
+        if (st != ESCAPED && st != CAPTURED) L.fails += 1;
+        if (st == ESCAPED) L.hi = L.mid; else L.lo = L.mid;
+        L.it += 1;
+        if (L.it < a.iterations) want = (st == ESCAPED) ? 1 : 0;
+        slot[lane] = -1;
+      }
+      __syncwarp();
+      const int hl = (role == EDGE_HELPER) ? host : (int)lane;
+      const int host_want = __shfl_sync(FULL, want, hl);
+      const bool host_ended = role == EDGE_HELPER && ((em >> hl) & 1u);
+      const bool on_side = host_ended && host_want >= 0 && ((path >> (depth - 1)) & 1) == host_want;
+      const bool heir = on_side && depth == 1;
+      if (heir) slot[host] = (int)lane;
+      __syncwarp();
+      const int my_heir = ended ? slot[lane] : -1;
+      const int new_host = host_ended ? slot[host] : -1;
+      const int src = heir ? host : (int)lane;
+      const double lo_s = __shfl_sync(FULL, L.lo, src);
+      const double hi_s = __shfl_sync(FULL, L.hi, src);
+      const long long fails_s = __shfl_sync(FULL, L.fails, src);
+      const long long g_s = __shfl_sync(FULL, g, src);
+      const int it_s = __shfl_sync(FULL, L.it, src);
+      if (heir) {  // the item's bracket is this lane's: its midpoint is this photon's
+        L.lo = lo_s;
+        L.hi = hi_s;
+        L.fails = fails_s;
+        L.it = it_s;
+        g = g_s;
+        role = EDGE_OWNER;
+      } else if (on_side) {  // one level up, below the heir (or the same owner)
+        depth -= 1;
+        path &= (1 << depth) - 1;
+        if (new_host >= 0) host = new_host;
+      } else if (host_ended) {  // the other side: the photon is not needed
+        my_discarded += (unsigned long long)L.ry.attempts;
+        role = EDGE_IDLE;
+      }
+      if (ended) {
+        if (want < 0) finish_item();
+        else if (my_heir >= 0) role = EDGE_IDLE;
+        else edge_start<M>(a, L);  // the next halving here (ends at once: next pass)
+      }
+      __syncwarp();
+    }
   };
   while (true) {
-    const unsigned idle = __ballot_sync(FULL, !active);
+    resolve();
+    // New items from the queue for idle lanes.
+    const unsigned idle = __ballot_sync(FULL, role == EDGE_IDLE);
     const int n_idle = __popc(idle);
     if (!drained && n_idle > 0 && (n_idle >= a.refill_threshold || n_idle == 32)) {
+      dirty = true;
       unsigned long long base = 0;
       const int leader = __ffs(idle) - 1;
       if ((int)lane == leader) base = atomicAdd(&a.q->head, (unsigned long long)n_idle);
       base = __shfl_sync(FULL, base, leader);
       if (base + (unsigned long long)n_idle >= (unsigned long long)a.n_items) drained = true;
-      if (!active) {
+      if (role == EDGE_IDLE) {
         const unsigned long long mine = base + (unsigned long long)__popc(idle & lt_mask);
         if (mine < (unsigned long long)a.n_items) {
-          g = (long long)mine;
+          g = a.order ? a.order[mine] : (long long)mine;
           L.c = a.item_case[g];
           L.lo = a.lo[g];
           L.hi = a.hi[g];
@@ -374,58 +483,136 @@ __global__ void __launch_bounds__(MAXT, MINB) k_bisect_edges(EdgeArgs a) {
           L.sphi = a.sin_phi[g];
           L.fails = 0;
           L.it = 0;
-          active = a.iterations > 0;
-          if (active) {
-            edge_start<M>(a, L);
-            while (active && L.ry.state != RUNNING) active = edge_next<M>(a, L);
-          }
-          if (!active) finish_item();
+          role = EDGE_OWNER;
+          if (a.iterations > 0) edge_start<M>(a, L);
+          else finish_item();
         }
       }
+      resolve();
     }
-    const unsigned busy = __ballot_sync(FULL, active);
+    // Once the queue is drained: idle lanes take the untraced nodes below the owners'
+    // brackets, shallowest first, then in lane order of the owners.
+    if (drained && dirty) {
+      dirty = false;
+      const unsigned idle2 = __ballot_sync(FULL, role == EDGE_IDLE);
+      if (idle2) {
+        slot[lane] = 0;
+        __syncwarp();
+        if (role == EDGE_HELPER) atomicOr(&slot[host], 1 << edge_node(depth, path));
+        __syncwarp();
+        const unsigned cover = (unsigned)slot[lane];
+        const int rank = (role == EDGE_IDLE) ? __popc(idle2 & lt_mask) : -1;
+        int h = -1, hd = 0, hp = 0, base_rank = 0;
+#pragma unroll
+        for (int d = 1; d <= EDGE_DEPTH; ++d) {
+          const int width = 1 << d;
+          unsigned seg = 0;
+          if (role == EDGE_OWNER && L.it + d < a.iterations)
+            seg = (~cover >> (width - 2)) & (width == 32 ? FULL : ((1u << width) - 1u));
+          const int cnt = __popc(seg);
+          int incl = cnt;
+#pragma unroll
+          for (int off = 1; off < 32; off <<= 1) {
+            const int t = __shfl_up_sync(FULL, incl, off);
+            if ((int)lane >= off) incl += t;
+          }
+          const int total = __shfl_sync(FULL, incl, 31);
+          const bool mine = h < 0 && rank >= base_rank && rank < base_rank + total;
+          const int key = mine ? rank - base_rank : -1;
+          int j = 0;  // the owner lane: the first with incl > key
+#pragma unroll
+          for (int step = 16; step >= 1; step >>= 1) {
+            const int v = __shfl_sync(FULL, incl, j + step - 1);
+            if (v <= key) j += step;
+          }
+          const int excl_j = __shfl_sync(FULL, incl - cnt, j);
+          const unsigned seg_j = __shfl_sync(FULL, seg, j);
+          if (mine) {
+            h = j;
+            hd = d;
+            hp = nth_set_bit(seg_j, key - excl_j);
+          }
+          base_rank += total;
+        }
+        const int src = (h >= 0) ? h : (int)lane;
+        double lo_s = __shfl_sync(FULL, L.lo, src);
+        double hi_s = __shfl_sync(FULL, L.hi, src);
+        const double cphi_s = __shfl_sync(FULL, L.cphi, src);
+        const double sphi_s = __shfl_sync(FULL, L.sphi, src);
+        const int c_s = __shfl_sync(FULL, L.c, src);
+        const int it_s = __shfl_sync(FULL, L.it, src);
+        if (h >= 0) {
+          // the brackets along the path from the owner's: escaped halves to [lo, mid]
+          for (int k = hd - 1; k >= 0; --k) {
+            const double mid = 0.5 * (lo_s + hi_s);
+            if ((hp >> k) & 1) hi_s = mid; else lo_s = mid;
+          }
+          L.lo = lo_s;
+          L.hi = hi_s;
+          L.cphi = cphi_s;
+          L.sphi = sphi_s;
+          L.c = c_s;
+          L.it = it_s + hd;
+          host = h;
+          depth = hd;
+          path = hp;
+          role = EDGE_HELPER;
+          my_spec += 1;
+          edge_start<M>(a, L);
+        }
+        __syncwarp();
+      }
+    }
+    const unsigned busy = __ballot_sync(FULL, role != EDGE_IDLE && L.ry.state == RUNNING);
     if (busy == 0) {
       if (drained) break;
       continue;
     }
     my_iters += 1;
-    if (active) {
-      attempt<M, false>(a.cases[L.c].P, L.ry, nullptr, nullptr);
-      if (L.ry.state != RUNNING) {
-        my_attempts += (unsigned long long)L.ry.attempts;
-        my_accepted += (unsigned long long)L.ry.n_steps;
-        bool more = edge_next<M>(a, L);
-        while (more && L.ry.state != RUNNING) more = edge_next<M>(a, L);
-        if (!more) finish_item();
-      }
+    if (role != EDGE_IDLE && L.ry.state == RUNNING) {
+      attempt<M, false>(params(L.c), L.ry, nullptr, nullptr);
+      my_attempts += 1;
     }
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     my_attempts += __shfl_down_sync(FULL, my_attempts, off);
     my_accepted += __shfl_down_sync(FULL, my_accepted, off);
+    my_spec += __shfl_down_sync(FULL, my_spec, off);
+    my_discarded += __shfl_down_sync(FULL, my_discarded, off);
   }
   if (lane == 0) {
     atomicAdd(&a.q->attempts, my_attempts);
     atomicAdd(&a.q->accepted, my_accepted);
     atomicAdd(&a.q->busy_iters, my_attempts);
     atomicAdd(&a.q->lane_iters, (unsigned long long)my_iters * 32ull);
+    atomicAdd(&a.q->speculative, my_spec);
+    atomicAdd(&a.q->discarded, my_discarded);
   }
 }
 
-template <class M, int MAXT, int MINB>
-cudaError_t run_bisect(EdgeArgs a, cudaStream_t s) {
-  if (a.n_items <= 0) return cudaSuccess;
+template <class M, int MAXT, int MINB, bool SMEM>
+cudaError_t run_bisect_as(EdgeArgs a, cudaStream_t s) {
+  const size_t smem = SMEM ? (size_t)a.n_cases * sizeof(Params) : 0;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bisect_edges<M, MAXT, MINB>, MAXT, 0) != cudaSuccess || nb < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bisect_edges<M, MAXT, MINB, SMEM>, MAXT, smem) !=
+          cudaSuccess ||
+      nb < 1)
     return cudaErrorLaunchOutOfResources;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   a.block = MAXT;
   a.grid = sms * nb;
-  k_bisect_edges<M, MAXT, MINB><<<a.grid, MAXT, 0, s>>>(a);
+  k_bisect_edges<M, MAXT, MINB, SMEM><<<a.grid, MAXT, smem, s>>>(a);
   return cudaGetLastError();
+}
+
+template <class M, int MAXT, int MINB>
+cudaError_t run_bisect(EdgeArgs a, cudaStream_t s) {
+  if (a.n_items <= 0) return cudaSuccess;
+  return edge_params_in_smem(a.n_cases) ? run_bisect_as<M, MAXT, MINB, true>(a, s)
+                                        : run_bisect_as<M, MAXT, MINB, false>(a, s);
 }
 
 // Flag the pixels whose classification the FP64 re-trace must settle: every photon that did not

@@ -380,6 +380,60 @@ def test_batched_edge_bisection_over_cases() -> None:
         assert e["rms_M"] < 20 * case.rtol, (case.spacetime.spin, e)
 
 
+def _sequential_bisection(case, iterations: int, backend):
+    """The reference's own loop (study_edge_bisection.py:53-68): one integrate_batch over every
+    direction per halving, on the same camera states and arithmetic as the batched kernel."""
+    from kerrray_b200.bisect import edge_options
+
+    integ, term = edge_options(case.rtol, case.r_o)
+    lo, hi = np.array(case.r_lo, dtype=np.float64), np.array(case.r_hi, dtype=np.float64)
+    lost = np.zeros(lo.size, dtype=np.int64)
+    cphi, sphi = np.cos(case.angles), np.sin(case.angles)
+    for _ in range(iterations):
+        mid = 0.5 * (lo + hi)
+        y0 = K.initial_states_at(case.spacetime, case.r_o, case.inclination_deg,
+                                 case.centre[0] + mid * cphi, case.centre[1] + mid * sphi)
+        st = np.asarray(backend.integrate_batch(case.spacetime, y0, integ, term).state)
+        lost += (st != 1) & (st != 2)
+        hi = np.where(st == 1, mid, hi)
+        lo = np.where(st == 1, lo, mid)
+    return 0.5 * (lo + hi), hi - lo, lost
+
+
+def test_bisection_tracing_ahead_is_the_sequential_bisection() -> None:
+    """Idle lanes trace midpoints ahead of their bracket (items of four cases interleaved, the
+    cases' parameters in shared memory); the brackets and lost-photon counts must still be
+    those of the plain sequential bisection, bit for bit."""
+    angles = 2 * np.pi * np.arange(48) / 48
+    cases = [K.edge_study(K.Spacetime(1.0, a), i, 1.0e4, rt, angles, bracket=(2.0, 8.0))
+             for a, i, rt in ((0.0, 17.0, 1e-5), (0.9, 60.0, 1e-6), (0.99, 85.0, 1e-7), (0.5, 40.0, 1e-8))]
+    iterations = 12
+    for precision in ("fast64", "reference"):
+        res, stats = K.bisect_edges(cases, iterations, precision=precision, item_failures=True)
+        assert stats["retired"] == 4 * 48
+        assert stats["speculative"] > 0 and stats["attempts"] < stats["busy_slots"], stats
+        backend = K.CudaBackend(precision=precision)
+        for case, (r_mid, width, fails) in zip(cases, res):
+            r2, w2, f2 = _sequential_bisection(case, iterations, backend)
+            assert np.array_equal(r2, r_mid) and np.array_equal(w2, width), (precision, case.rtol)
+            assert np.array_equal(f2, fails)
+
+
+def test_bisection_with_many_cases_is_the_sequential_bisection() -> None:
+    """More cases than shared memory holds (their parameters stay in global memory, the items
+    in the caller's order): the same bit-for-bit agreement with the sequential bisection."""
+    angles = np.array([0.3, 2.5])
+    cases = [K.EdgeCase(K.Spacetime(1.0, 0.5 + 1e-3 * k), 60.0, 1.0e3, 1e-6, (0.1, -0.2), angles,
+                        np.full(2, 2.0), np.full(2, 8.0)) for k in range(300)]
+    iterations = 4
+    res, stats = K.bisect_edges(cases, iterations, precision="fast64", item_failures=True)
+    assert stats["retired"] == 600
+    backend = K.CudaBackend(precision="fast64")
+    for case, (r_mid, width, fails) in list(zip(cases, res))[::7]:
+        r2, w2, f2 = _sequential_bisection(case, iterations, backend)
+        assert np.array_equal(r2, r_mid) and np.array_equal(w2, width) and np.array_equal(f2, fails)
+
+
 def test_exact_checks_on_the_cuda_backend() -> None:
     """The reference's Schwarzschild exact checks (configs/schwarzschild.yaml settings: rtol 1e-9,
     atol 1e-11, 15 probes per iteration, brackets [2.5, 4] M and [4, 7] M, tolerance 1e-6 M):
