@@ -76,8 +76,9 @@ class CudaBackend:
         device: CUDA device ordinal.
         precision: ``"reference"`` (default; the reference's operation order in FP64, or its
             float32 mode when ``integ.dtype == "float32"``), ``"fast64"`` (FP64 with FMA,
-            sincos and reciprocals) or ``"mixed"`` (FP32 stages with FP64 accumulation,
-            Delta and error norm; rk45 only).
+            sincos and Newton reciprocals good to 2^-40 relative; for rtol below about 1e-11
+            use ``"reference"``) or ``"mixed"`` (FP32 stages with FP64 accumulation, Delta and
+            error norm; rk45 only).
 
     Raises:
         BackendUnavailable: When the library, the driver or the device is missing.

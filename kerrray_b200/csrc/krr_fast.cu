@@ -3,6 +3,8 @@
 // fuses nothing else and every launch variant (register cap) computes identical results.
 #include <math_constants.h>
 
+#include <algorithm>
+
 #include "krr_launch.h"
 
 namespace krr {
@@ -163,6 +165,23 @@ cudaError_t trig_eval(int which, const double* theta, const double* delta, long 
   if (n <= 0) return cudaSuccess;
   const int block = 256;
   k_trig_eval<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(which, theta, delta, n, s_out, c_out);
+  return cudaGetLastError();
+}
+
+// Count of the non-finite values among n doubles (added to *count).
+__global__ void k_count_nonfinite(const double* __restrict__ x, long long n, unsigned long long* count) {
+  unsigned long long mine = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) mine += !isfinite(x[i]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, off);
+  if ((threadIdx.x & 31u) == 0 && mine) atomicAdd(count, mine);
+}
+
+cudaError_t count_nonfinite(const double* x, long long n, unsigned long long* count, int sms, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((n + 255) / 256, (long long)std::max(sms, 1) * 8);
+  k_count_nonfinite<<<(unsigned)blocks, 256, 0, s>>>(x, n, count);
   return cudaGetLastError();
 }
 

@@ -23,6 +23,9 @@ const Variant* mixed_sat_variant();
 cudaError_t escape_directions(const Params& P, double r_s, const double* Y, const long long* state, long long n,
                               double* theta, double* phi, cudaStream_t s);
 
+// Adds to *count (device) the number of non-finite values among the n doubles at x (device).
+cudaError_t count_nonfinite(const double* x, long long n, unsigned long long* count, int sms, cudaStream_t s);
+
 // The step kernels' sine and cosine forms at given angles (which: 0 FP32 reduced, 1 FP32 shift,
 // 2 FP64 shift; see k_trig_eval).
 cudaError_t trig_eval(int which, const double* theta, const double* delta, long long n, double* s_out, double* c_out,

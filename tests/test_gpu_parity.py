@@ -227,6 +227,15 @@ def test_empty_batch_and_input_errors() -> None:
                                                          K.TerminationOptions())
     with pytest.raises(ValueError):
         K.initial_states(K.Camera(radius=1.4, inclination_deg=60.0, fov=0.1, resolution=2), st)
+    # trace_images checks a host Y0 on the device, before any trace work
+    spec = K.ImageSpec(st, K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=8),
+                       K.IntegratorOptions(), K.TerminationOptions())
+    y0 = K.initial_states(spec.camera, st)
+    y0[17, 5] = np.inf
+    with pytest.raises(ValueError, match="finite"):
+        K.trace_images([spec], Y0=y0)
+    y0[17, 5] = 0.0
+    assert K.trace_images([spec], Y0=y0).arrays["state"].shape == (64,)
 
 
 def test_every_launch_variant_gives_identical_results() -> None:
