@@ -198,6 +198,8 @@ struct Context {
   int device = -1;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  cudaStream_t copy_stream = nullptr;   // device-to-host copies beside the trace (krr_trace_images)
+  cudaEvent_t chunk_ev[4] = {};         // the end of each chunk's trace
   int sm_count = 0;
   DevBuf buf[B_COUNT];
 };
@@ -221,6 +223,8 @@ int get_context(int device, Context** out) {
     KRR_CUDA(cudaEventCreate(&c->ev0));
     KRR_CUDA(cudaEventCreate(&c->ev1));
     KRR_CUDA(cudaEventCreate(&c->ev2));
+    KRR_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (auto& ev : c->chunk_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     KRR_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
     g_ctx[device] = std::move(c);
   }
@@ -336,6 +340,24 @@ int copy_results_back(Context* c, int64_t n, const krr_result* dev, const krr_re
   };
   for (auto& p : pairs)
     if (p.dst && p.src && p.bytes) KRR_CUDA(cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyDeviceToHost, c->stream));
+  return KRR_OK;
+}
+
+// Rows [r0, r1) of every requested result, device to host, on stream s.
+int copy_rows_back(const krr_result* dev, const krr_result* host, long long r0, long long r1, cudaStream_t s) {
+  const size_t n = (size_t)(r1 - r0), o = (size_t)r0;
+  struct Slice { void* dst; const void* src; size_t row; };
+  Slice sl[] = {
+      {host->Y, dev->Y, 64}, {host->state, dev->state, 8}, {host->n_steps, dev->n_steps, 8},
+      {host->n_rejected, dev->n_rejected, 8}, {host->lam, dev->lam, 8}, {host->max_null_error, dev->max_null_error, 8},
+      {host->max_energy_drift, dev->max_energy_drift, 8}, {host->max_lz_drift, dev->max_lz_drift, 8},
+      {host->max_carter_drift, dev->max_carter_drift, 8}, {host->event_Y, dev->event_Y, 64},
+      {host->event_hit, dev->event_hit, 1},
+  };
+  for (auto& x : sl)
+    if (x.dst && x.src && n)
+      KRR_CUDA(cudaMemcpyAsync(static_cast<char*>(x.dst) + o * x.row, static_cast<const char*>(x.src) + o * x.row,
+                               n * x.row, cudaMemcpyDeviceToHost, s));
   return KRR_OK;
 }
 
@@ -673,6 +695,78 @@ int run_images(Context* c, const krr_image* images, const std::vector<krr::Image
   KRR_CUDA(cudaMemcpyAsync(p.w.images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, s));
   KRR_CUDA(enqueue_pipeline(p, s, c->ev0, c->ev1, c->ev2));
   return finish_pipeline(p, s, stats, c->ev0, c->ev1, c->ev2);
+}
+
+// krr_trace_images with host results and no re-trace: the photons in up to four consecutive
+// ranges, one persistent launch each (queue k starts at its range's first photon), each
+// range's results copied to the host on a second stream while the next range is traced.  The
+// copies (1.6 GB for the 12.4M-photon sweep) then hide behind the trace except the last
+// range's; each extra launch costs one tail of idle lanes.
+constexpr long long kChunkPhotons = 2'000'000;  // ranges of at least this many photons
+
+int run_images_overlapped(Context* c, const krr_image* images, const std::vector<krr::Image>& ims, long long total,
+                          const double* d_Y0, const krr_launch* launch, const krr_result* d_out,
+                          const krr_result* host_out, void* d_work, size_t work_size, krr_stats* stats) {
+  Pipeline p;
+  int rc = prepare_pipeline(c->device, images, (int)ims.size(), total, d_Y0, launch, d_out, d_work, work_size, p);
+  if (rc) return rc;
+  const cudaStream_t s = c->stream;
+  const int chunks = (int)std::min<long long>(4, std::max<long long>(1, total / kChunkPhotons));
+  krr::Queue* qs[4] = {p.w.q0, p.w.q1, p.w.q2, p.w.q3};
+  krr::Queue init[4];
+  std::memset(init, 0, sizeof(init));
+  long long bound[5];
+  for (int k = 0; k <= chunks; ++k) bound[k] = total * k / chunks;
+  KRR_CUDA(cudaMemcpyAsync(p.w.images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, s));
+  KRR_CUDA(cudaMemsetAsync(p.w.q0, 0, kQueueArea, s));
+  for (int k = 0; k < chunks; ++k) {
+    init[k].head = (unsigned long long)bound[k];
+    KRR_CUDA(cudaMemcpyAsync(qs[k], &init[k], sizeof(krr::Queue), cudaMemcpyHostToDevice, s));
+  }
+  if (p.out.event_Y) KRR_CUDA(cudaMemsetAsync(p.out.event_Y, 0, (size_t)total * 8 * sizeof(double), s));
+  if (p.out.event_hit) KRR_CUDA(cudaMemsetAsync(p.out.event_hit, 0, (size_t)total, s));
+  KRR_CUDA(cudaEventRecord(c->ev0, s));
+  for (int k = 0; k < chunks; ++k) {
+    krr::PersistArgs a = p.main;
+    a.q = qs[k];
+    a.total = bound[k + 1];
+    KRR_CUDA(p.main_v->run(a, s));
+    KRR_CUDA(cudaEventRecord(c->chunk_ev[k], s));
+    KRR_CUDA(cudaStreamWaitEvent(c->copy_stream, c->chunk_ev[k], 0));
+    rc = copy_rows_back(d_out, host_out, bound[k], bound[k + 1], c->copy_stream);
+    if (rc) return rc;
+  }
+  KRR_CUDA(cudaEventRecord(c->ev1, s));
+  krr::Queue q[4];
+  std::memset(q, 0, sizeof(q));
+  for (int k = 0; k < chunks; ++k) KRR_CUDA(cudaMemcpyAsync(&q[k], qs[k], sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaStreamSynchronize(s));
+  KRR_CUDA(cudaStreamSynchronize(c->copy_stream));
+  float ms = 0.0f;
+  KRR_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  krr::Queue sum{};
+  for (int k = 0; k < chunks; ++k) {
+    if (q[k].error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
+    if (q[k].retired != (unsigned long long)(bound[k + 1] - bound[k]))
+      return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu photons retired of %lld in range %d", q[k].retired,
+                  bound[k + 1] - bound[k], k);
+    sum.retired += q[k].retired;
+    sum.attempts += q[k].attempts;
+    sum.accepted += q[k].accepted;
+    sum.lane_iters += q[k].lane_iters;
+    sum.busy_iters += q[k].busy_iters;
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->photons = (uint64_t)total;
+    stats->retired = sum.retired;
+    stats->attempts = sum.attempts;
+    stats->accepted = sum.accepted;
+    stats->lane_slots = sum.lane_iters;
+    stats->busy_slots = sum.busy_iters;
+    stats->kernel_ms = ms;
+  }
+  return KRR_OK;
 }
 
 }  // namespace krr_host
@@ -1215,6 +1309,8 @@ int krr_trace_images(int device, const krr_image* images, int32_t n_images, cons
   if (rc) return rc;
   const size_t wbytes = work_bytes(n_images, (launch && launch->retrace) ? total : 0);
   KRR_CUDA(c->buf[B_QUEUE].ensure(wbytes));
+  if (total >= 2 * kChunkPhotons && !(launch && (launch->retrace || launch->plain)))
+    return run_images_overlapped(c, images, ims, total, d_Y0, launch, &dev, out, c->buf[B_QUEUE].p, wbytes, stats);
   rc = run_images(c, images, ims, total, d_Y0, launch, &dev, c->buf[B_QUEUE].p, wbytes, c->stream, stats);
   if (rc) return rc;
   rc = copy_results_back(c, total, &dev, out);

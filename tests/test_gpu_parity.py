@@ -443,6 +443,22 @@ def test_bisection_with_many_cases_is_the_sequential_bisection() -> None:
         assert np.array_equal(r2, r_mid) and np.array_equal(w2, width) and np.array_equal(f2, fails)
 
 
+def test_trace_images_with_overlapped_copies_is_one_launch() -> None:
+    """With more than 4M photons, trace_images traces four consecutive ranges and copies each
+    range's results to the host while the next one is traced; the results are those of one
+    launch over all photons (the device-resident sweep), bit for bit."""
+    spec = K.ImageSpec(K.Spacetime(1.0, 0.9), K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=2048),
+                       K.IntegratorOptions(rtol=1e-5, atol=1e-7), K.TerminationOptions())
+    launch = K.LaunchConfig(variant=1, refill_threshold=4)
+    host = K.trace_images([spec], precision="fast64", launch=launch)
+    assert host.stats["retired"] == 2048 * 2048
+    dev = K.DeviceSweep([spec], precision="fast64", launch=launch)
+    dev.run()
+    for name in ("state", "Y", "n_steps", "n_rejected", "lam", "max_null_error"):
+        assert np.array_equal(host.arrays[name], dev.tensors[name].cpu().numpy()), name
+    dev.close()
+
+
 def test_exact_checks_on_the_cuda_backend() -> None:
     """The reference's Schwarzschild exact checks (configs/schwarzschild.yaml settings: rtol 1e-9,
     atol 1e-11, 15 probes per iteration, brackets [2.5, 4] M and [4, 7] M, tolerance 1e-6 M):
