@@ -8,8 +8,10 @@ classification on the device). Metric: rays/s, the whole job over all ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun every rank traces the full sweep on its own GPU (weak scaling; the photons are
-independent, there is no data-path collective); the time is the max over ranks.
+Under torchrun the job is N copies of the sweep with the observer turned in azimuth (distinct
+images of equal cost), split across the N ranks by predicted cost (kerrray_b200.shard): each
+rank traces one sweep's worth on its own GPU (weak scaling; the photons are independent, there
+is no data-path collective); the time is the max over ranks.
 ``--impl reference`` times the CPU restatement of the reference kernel (the oracle, OpenMP over
 all host threads) on a bounded sample of the same workload.
 """
@@ -308,7 +310,11 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024") -> d
         sw.run()
     t = {k: min(_timed_steps(sw, 3 if k != "plain" else 2, stream, flush))
          for k, sw in zip(("crit", "edge", "bare", "fast", "plain"), sweeps)}
-    cs, es = crit.stats(), edge.stats()
+    cs, es, bs = crit.stats(), edge.stats(), bare.stats()
+    from kerrray_b200 import _lib
+
+    mixed_tflops = algorithmic_flops(bs) / (t["bare"] * 1e-3) / 1e12
+    peak32, peak64 = _lib.fma_peak_tflops(local, False), _lib.fma_peak_tflops(local, True)
     ref = plain.tensors["state"]
     esc = (ref == 1) & (crit.tensors["state"] == 1)
     # Terminal states compared where each escaped ray crosses the escape surface: the final
@@ -330,6 +336,12 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024") -> d
            "pipeline": "analytic critical set in reference-order FP64 beside the mixed trace, then a re-trace of "
                        "every photon unlike its analytic class",
            "mixed_kernel_only_rays_s": total / (t["bare"] * 1e-3),
+           "mixed_kernel_roofline": {"achieved": mixed_tflops, "unit": "TFLOP/s", "fp32_peak": peak32,
+                                     "frac_fp32": mixed_tflops / peak32, "fp64_peak": peak64,
+                                     "attempts": int(bs["attempts"]), "accepted": int(bs["accepted"]),
+                                     "note": "the reference's algorithmic FLOPs per second of the mixed kernel "
+                                             "(stages in FP32, accumulation and error norm in FP64) against the "
+                                             "measured FP32 and FP64 FMA peaks"},
            "mixed_edge_retrace_rays_s": total / (t["edge"] * 1e-3),
            "edge_retrace_mask_identical": bool(torch.equal(edge.tensors["state"], ref)),
            "edge_retraced": int(es["retraced"]),
@@ -360,11 +372,15 @@ def run_ours(args) -> None:
     if world > 1:
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     _lib.lib()
 
-    specs = workload_specs(K, args.workload)
-    total = sum(s.n_rays for s in specs)
+    from kerrray_b200 import shard
+
+    specs_all = shard.replicate_specs(workload_specs(K, args.workload), world)
+    specs = [specs_all[k] for k in shard.shard_specs(specs_all, rank, world)]
+    total = sum(s.n_rays for s in specs)              # this rank's photons
+    job_total = sum(s.n_rays for s in specs_all)      # every rank's
     if args.launch:
         variant, refill = (int(x) for x in args.launch.split(":"))
         tuned = K.LaunchConfig(variant=variant, refill_threshold=refill)
@@ -391,12 +407,8 @@ def run_ours(args) -> None:
         barrier()
     clock = clocks.summary()
     stats = sweep.stats()
-    elapsed_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
-    value = world * total * args.steps / (elapsed_ms / 1e3)
+    elapsed_ms = shard.max_over_ranks(float(sum(step_ms)))
+    value = job_total * args.steps / (elapsed_ms / 1e3)
 
     # Roofline of the trace kernel: algorithmic FLOPs per launch over its event-timed duration
     # (each timed graph launch holds this one kernel and two small memsets).
@@ -448,7 +460,7 @@ def run_ours(args) -> None:
             K.trace_images(specs, precision=args.precision, Y0=y0, out=outs, device=local, launch=tuned)
         e2e_s = (time.perf_counter() - t0) / e2e_steps
         d2h = sum(a.nbytes for a in outs.values() if a is not None)
-        e2e = {"value": world * total / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": int(y0.nbytes),
+        e2e = {"value": job_total / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": int(y0.nbytes),
                "d2h_bytes_per_step": int(d2h)}
         counts = np.bincount(outs["state"], minlength=7)
         extra["state_counts"] = {n: int(c) for n, c in zip(
@@ -462,9 +474,10 @@ def run_ours(args) -> None:
             "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload], "photons": total, "images": len(specs),
-                       "precision": args.precision, "kernel": "persistent work queue, CUDA-graph launch",
-                       "parallelism": f"replicas{world}",
+            "config": {"workload": WORKLOADS[args.workload], "photons": job_total, "images": len(specs_all),
+                       "photons_per_gpu": total, "precision": args.precision,
+                       "kernel": "persistent work queue, CUDA-graph launch",
+                       "parallelism": f"shards{world} (images split by predicted cost; no data-path collective)",
                        "launch": {k: v for k, v in chosen.items() if k != "ms"},
                        "l2": "256 MB buffer written between timed steps (> 126 MB L2)"},
             "e2e": e2e, "gpu_launches": args.steps,
