@@ -360,7 +360,7 @@ __device__ __forceinline__ int nth_set_bit(unsigned mask, int n) {
 // items of different cases, and each parameter load is then one shared-memory access (the
 // 184-byte stride, 23 doubles, is odd: no bank conflicts) instead of one global-memory
 // wavefront per distinct case.
-constexpr size_t kEdgeSmemMax = 48 * 1024;
+constexpr size_t kEdgeSmemMax = 46 * 1024;  // within the 48 KB a block gets without opt-in, beside its static slots
 __host__ __device__ constexpr bool edge_params_in_smem(int n_cases) {
   return (size_t)n_cases * sizeof(Params) <= kEdgeSmemMax;
 }
