@@ -697,7 +697,14 @@ __device__ __forceinline__ typename M::N step_factor_sq(typename M::N en2, bool 
   using N = typename M::N;
   N factor = (N)FACTOR_MAX;
   if (en2 != (N)0.0) {
-    const N raw = (N)(0.9f * exp2f(-0.1f * __log2f((float)en2)));
+    float lg, ex;
+    if constexpr (M::kMixed) {  // the bare hardware approximations (subnormals flush to zero): +1 %
+      asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(lg) : "f"((float)en2));
+      asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ex) : "f"(-0.1f * lg));
+    } else {
+      ex = exp2f(-0.1f * __log2f((float)en2));
+    }
+    const N raw = (N)(0.9f * ex);
     factor = py_min((N)FACTOR_MAX, py_max((N)FACTOR_MIN, raw));
   }
   if (rejected_before) factor = py_min(factor, (N)1.0);
