@@ -259,6 +259,31 @@ def _timed_steps(sweep, steps: int, stream, flush) -> list[float]:
     return out
 
 
+PLAIN_BLOCKS = (32, 64, 128, 256)
+
+
+def best_plain(K, specs, local: int, stream, flush, steps: int):
+    """The plain FP64 kernel (one thread per photon, reference operation order) at its fastest
+    block size: each of PLAIN_BLOCKS timed once, the fastest again over ``steps`` launches.
+    Returns (its DeviceSweep, best ms, block, ms per block). The results do not depend on the
+    block size (the arithmetic is per photon)."""
+    import torch
+
+    by_block = {}
+    for blk in PLAIN_BLOCKS:
+        sw = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True, block=blk))
+        sw.run(stats=False)
+        by_block[blk] = min(_timed_steps(sw, 1, stream, flush))
+        sw.close()
+        del sw
+        torch.cuda.empty_cache()
+    blk = min(by_block, key=by_block.get)
+    sw = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True, block=blk))
+    sw.run(stats=False)
+    best = min([by_block[blk]] + _timed_steps(sw, steps, stream, flush))
+    return sw, best, blk, {str(b): round(t, 3) for b, t in by_block.items()}
+
+
 def edge_rms_px(K, spec, state: np.ndarray) -> float:
     """rms distance (px) of the captured-mask edge from Bardeen's curve after the finite-distance
     correction (``raytracing/boundary.py``: 1/8-px marching of the bilinear 0.5 level set)."""
@@ -304,12 +329,11 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024") -> d
 
     crit, edge, bare = mixed_with(K.RETRACE_CRITICAL), mixed_with(K.RETRACE_EDGE), mixed_with(0)
     fast = K.DeviceSweep(specs, precision="fast64", device=local, launch=K.autotune(specs, precision="fast64", device=local)[0])
-    plain = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True))
-    sweeps = (crit, edge, bare, fast, plain)
+    sweeps = (crit, edge, bare, fast)
     for sw in sweeps:
         sw.run()
-    t = {k: min(_timed_steps(sw, 3 if k != "plain" else 2, stream, flush))
-         for k, sw in zip(("crit", "edge", "bare", "fast", "plain"), sweeps)}
+    t = {k: min(_timed_steps(sw, 3, stream, flush)) for k, sw in zip(("crit", "edge", "bare", "fast"), sweeps)}
+    plain, t["plain"], plain_block, plain_by_block = best_plain(K, specs, local, stream, flush, 2)
     cs, es, bs = crit.stats(), edge.stats(), bare.stats()
     from kerrray_b200 import _lib
 
@@ -329,6 +353,7 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024") -> d
     st_mixed = crit.tensors["state"].cpu().numpy()
     out = {"workload": WORKLOADS[name], "photons": total,
            "mixed_pipeline_rays_s": total / (t["crit"] * 1e-3), "plain_fp64_rays_s": total / (t["plain"] * 1e-3),
+           "plain_fp64_block": plain_block, "plain_fp64_ms_by_block": plain_by_block,
            "speedup_mixed_vs_plain": t["plain"] / t["crit"],
            "mask_identical": bool(torch.equal(crit.tensors["state"], ref)),
            "pixels_differing": int((crit.tensors["state"] != ref).sum().item()),
@@ -421,10 +446,10 @@ def run_ours(args) -> None:
     e2e = None
     if rank == 0 and not args.kernel_only:
         # Plain FP64 (one thread per photon, reference operation order) on the same images.
-        plain = K.DeviceSweep(specs, precision="reference", device=local, launch=K.LaunchConfig(plain=True))
-        plain.run(stats=False)
-        t_plain = min(_timed_steps(plain, 1, stream, flush))
+        plain, t_plain, plain_block, plain_by_block = best_plain(K, specs, local, stream, flush, 1)
         extra["plain_fp64_rays_s"] = total / (t_plain * 1e-3)
+        extra["plain_fp64_block"] = plain_block
+        extra["plain_fp64_ms_by_block"] = plain_by_block
         extra["persistent_rays_s"] = total / (kernel_ms * 1e-3)
         extra["speedup_persistent_vs_plain"] = t_plain / kernel_ms
         extra["mask_identical_persistent_vs_plain"] = bool(torch.equal(plain.tensors["state"], sweep.tensors["state"]))
