@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -199,7 +200,9 @@ struct Context {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   cudaStream_t copy_stream = nullptr;   // device-to-host copies beside the trace (krr_trace_images)
+  cudaStream_t h2d_stream = nullptr;    // host-to-device copies of Y0 ahead of the trace
   cudaEvent_t chunk_ev[4] = {};         // the end of each chunk's trace
+  cudaEvent_t h2d_ev[4] = {};           // each chunk's Y0 on the device
   int sm_count = 0;
   DevBuf buf[B_COUNT];
 };
@@ -224,7 +227,9 @@ int get_context(int device, Context** out) {
     KRR_CUDA(cudaEventCreate(&c->ev1));
     KRR_CUDA(cudaEventCreate(&c->ev2));
     KRR_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    KRR_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
     for (auto& ev : c->chunk_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (auto& ev : c->h2d_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     KRR_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
     g_ctx[device] = std::move(c);
   }
@@ -240,6 +245,22 @@ bool all_finite(const double* x, size_t n) {
   uint64_t bad = 0;
   for (size_t i = 0; i < n; ++i) bad |= (uint64_t)((b[i] & kExp) == kExp);
   return bad == 0;
+}
+
+// all_finite over up to 16 host threads for large arrays (memory-bandwidth bound).
+bool all_finite_parallel(const double* x, size_t n) {
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (n < ((size_t)1 << 22) || hw == 1) return all_finite(x, n);
+  std::vector<char> ok(hw, 1);
+  std::vector<std::thread> threads;
+  const size_t per = (n + hw - 1) / hw;
+  for (unsigned t = 0; t < hw; ++t)
+    threads.emplace_back([&, t] {
+      const size_t a = t * per, b = std::min(n, a + per);
+      if (a < b) ok[t] = all_finite(x + a, b - a);
+    });
+  for (auto& th : threads) th.join();
+  return std::all_of(ok.begin(), ok.end(), [](char v) { return v != 0; });
 }
 
 // Host Y0 (rows x 8) to the device buffer B_Y0, checked there for non-finite values before any
@@ -699,24 +720,47 @@ int run_images(Context* c, const krr_image* images, const std::vector<krr::Image
 
 // krr_trace_images with host results and no re-trace: the photons in up to four consecutive
 // ranges, one persistent launch each (queue k starts at its range's first photon), each
-// range's results copied to the host on a second stream while the next range is traced.  The
-// copies (1.6 GB for the 12.4M-photon sweep) then hide behind the trace except the last
-// range's; each extra launch costs one tail of idle lanes.
+// range's results copied to the host on a second stream while the next range is traced, and a
+// host Y0 copied in range by range on a third.  The copies (0.8 GB in, 1.6 GB out for the
+// 12.4M-photon sweep) then hide behind the trace except the first range's input and the last
+// range's output; each extra launch costs one tail of idle lanes.
 constexpr long long kChunkPhotons = 2'000'000;  // ranges of at least this many photons
 
 int run_images_overlapped(Context* c, const krr_image* images, const std::vector<krr::Image>& ims, long long total,
-                          const double* d_Y0, const krr_launch* launch, const krr_result* d_out,
+                          const double* host_Y0, const krr_launch* launch, const krr_result* d_out,
                           const krr_result* host_out, void* d_work, size_t work_size, krr_stats* stats) {
-  Pipeline p;
-  int rc = prepare_pipeline(c->device, images, (int)ims.size(), total, d_Y0, launch, d_out, d_work, work_size, p);
-  if (rc) return rc;
   const cudaStream_t s = c->stream;
   const int chunks = (int)std::min<long long>(4, std::max<long long>(1, total / kChunkPhotons));
+  // Ranges weighted 3:3:...:1: the last range's copy-out is the one not hidden behind a trace.
+  long long bound[5];
+  const long long wsum = 3LL * (chunks - 1) + 1;
+  for (int k = 0; k <= chunks; ++k) bound[k] = (k == chunks) ? total : total * (3LL * k) / wsum;
+  // A host Y0 goes up range by range on its own stream while the host checks it (every value
+  // finite) in parallel; no trace starts before the check has passed.
+  const double* d_Y0 = nullptr;
+  if (host_Y0) {
+    KRR_CUDA(c->buf[B_Y0].ensure((size_t)total * 8 * sizeof(double)));
+    double* dst = static_cast<double*>(c->buf[B_Y0].p);
+    for (int k = 0; k < chunks; ++k) {
+      const size_t off = (size_t)bound[k] * 8, n = (size_t)(bound[k + 1] - bound[k]) * 8;
+      KRR_CUDA(cudaMemcpyAsync(dst + off, host_Y0 + off, n * sizeof(double), cudaMemcpyHostToDevice, c->h2d_stream));
+      KRR_CUDA(cudaEventRecord(c->h2d_ev[k], c->h2d_stream));
+    }
+    if (!all_finite_parallel(host_Y0, (size_t)total * 8)) {
+      KRR_CUDA(cudaStreamSynchronize(c->h2d_stream));  // no copy may still read the caller's Y0
+      return fail(KRR_ERR_INVALID, "Y0 must be finite");
+    }
+    d_Y0 = dst;
+  }
+  Pipeline p;
+  int rc = prepare_pipeline(c->device, images, (int)ims.size(), total, d_Y0, launch, d_out, d_work, work_size, p);
+  if (rc) {
+    KRR_CUDA(cudaStreamSynchronize(c->h2d_stream));
+    return rc;
+  }
   krr::Queue* qs[4] = {p.w.q0, p.w.q1, p.w.q2, p.w.q3};
   krr::Queue init[4];
   std::memset(init, 0, sizeof(init));
-  long long bound[5];
-  for (int k = 0; k <= chunks; ++k) bound[k] = total * k / chunks;
   KRR_CUDA(cudaMemcpyAsync(p.w.images, ims.data(), ims.size() * sizeof(krr::Image), cudaMemcpyHostToDevice, s));
   KRR_CUDA(cudaMemsetAsync(p.w.q0, 0, kQueueArea, s));
   for (int k = 0; k < chunks; ++k) {
@@ -730,6 +774,7 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
     krr::PersistArgs a = p.main;
     a.q = qs[k];
     a.total = bound[k + 1];
+    if (host_Y0) KRR_CUDA(cudaStreamWaitEvent(s, c->h2d_ev[k], 0));
     KRR_CUDA(p.main_v->run(a, s));
     KRR_CUDA(cudaEventRecord(c->chunk_ev[k], s));
     KRR_CUDA(cudaStreamWaitEvent(c->copy_stream, c->chunk_ev[k], 0));
@@ -742,6 +787,7 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
   for (int k = 0; k < chunks; ++k) KRR_CUDA(cudaMemcpyAsync(&q[k], qs[k], sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaStreamSynchronize(s));
   KRR_CUDA(cudaStreamSynchronize(c->copy_stream));
+  KRR_CUDA(cudaStreamSynchronize(c->h2d_stream));
   float ms = 0.0f;
   KRR_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   krr::Queue sum{};
@@ -1299,8 +1345,9 @@ int krr_trace_images(int device, const krr_image* images, int32_t n_images, cons
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(c->mu);
   KRR_CUDA(cudaSetDevice(device));
+  const bool overlapped = total >= 2 * kChunkPhotons && !(launch && (launch->retrace || launch->plain));
   const double* d_Y0 = nullptr;
-  if (Y0) {
+  if (Y0 && !overlapped) {
     rc = upload_y0(c, Y0, total, &d_Y0);
     if (rc) return rc;
   }
@@ -1309,8 +1356,8 @@ int krr_trace_images(int device, const krr_image* images, int32_t n_images, cons
   if (rc) return rc;
   const size_t wbytes = work_bytes(n_images, (launch && launch->retrace) ? total : 0);
   KRR_CUDA(c->buf[B_QUEUE].ensure(wbytes));
-  if (total >= 2 * kChunkPhotons && !(launch && (launch->retrace || launch->plain)))
-    return run_images_overlapped(c, images, ims, total, d_Y0, launch, &dev, out, c->buf[B_QUEUE].p, wbytes, stats);
+  if (overlapped)
+    return run_images_overlapped(c, images, ims, total, Y0, launch, &dev, out, c->buf[B_QUEUE].p, wbytes, stats);
   rc = run_images(c, images, ims, total, d_Y0, launch, &dev, c->buf[B_QUEUE].p, wbytes, c->stream, stats);
   if (rc) return rc;
   rc = copy_results_back(c, total, &dev, out);

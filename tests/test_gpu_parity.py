@@ -456,6 +456,14 @@ def test_trace_images_with_overlapped_copies_is_one_launch() -> None:
     dev.run()
     for name in ("state", "Y", "n_steps", "n_rejected", "lam", "max_null_error"):
         assert np.array_equal(host.arrays[name], dev.tensors[name].cpu().numpy()), name
+    # a host Y0 goes up range by range, checked on the host before any range is traced
+    y0 = K.initial_states(spec.camera, spec.spacetime)
+    from_y0 = K.trace_images([spec], precision="fast64", launch=launch, Y0=y0)
+    assert np.array_equal(from_y0.arrays["state"], host.arrays["state"])
+    assert np.array_equal(from_y0.arrays["Y"], host.arrays["Y"])
+    y0[3_000_000, 6] = np.nan
+    with pytest.raises(ValueError, match="finite"):
+        K.trace_images([spec], precision="fast64", launch=launch, Y0=y0)
     dev.close()
 
 
