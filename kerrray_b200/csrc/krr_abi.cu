@@ -777,11 +777,15 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
     if (host_Y0) KRR_CUDA(cudaStreamWaitEvent(s, c->h2d_ev[k], 0));
     KRR_CUDA(p.main_v->run(a, s));
     KRR_CUDA(cudaEventRecord(c->chunk_ev[k], s));
+  }
+  KRR_CUDA(cudaEventRecord(c->ev1, s));
+  // Every launch is queued before the first copy-out: a copy into pageable host memory returns
+  // only when it has finished, and must not hold back the next range's launch.
+  for (int k = 0; k < chunks; ++k) {
     KRR_CUDA(cudaStreamWaitEvent(c->copy_stream, c->chunk_ev[k], 0));
     rc = copy_rows_back(d_out, host_out, bound[k], bound[k + 1], c->copy_stream);
     if (rc) return rc;
   }
-  KRR_CUDA(cudaEventRecord(c->ev1, s));
   krr::Queue q[4];
   std::memset(q, 0, sizeof(q));
   for (int k = 0; k < chunks; ++k) KRR_CUDA(cudaMemcpyAsync(&q[k], qs[k], sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
