@@ -730,6 +730,15 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
                           const double* host_Y0, const krr_launch* launch, const krr_result* d_out,
                           const krr_result* host_out, void* d_work, size_t work_size, krr_stats* stats) {
   const cudaStream_t s = c->stream;
+  // Whatever path returns, no copy may still read or write the caller's buffers afterwards.
+  struct Drain {
+    cudaStream_t trace, out, in;
+    ~Drain() {
+      cudaStreamSynchronize(trace);
+      cudaStreamSynchronize(out);
+      cudaStreamSynchronize(in);
+    }
+  } drain{s, c->copy_stream, c->h2d_stream};
   const int chunks = (int)std::min<long long>(4, std::max<long long>(1, total / kChunkPhotons));
   // Ranges weighted 3:3:...:1: the last range's copy-out is the one not hidden behind a trace.
   long long bound[5];
@@ -746,18 +755,12 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
       KRR_CUDA(cudaMemcpyAsync(dst + off, host_Y0 + off, n * sizeof(double), cudaMemcpyHostToDevice, c->h2d_stream));
       KRR_CUDA(cudaEventRecord(c->h2d_ev[k], c->h2d_stream));
     }
-    if (!all_finite_parallel(host_Y0, (size_t)total * 8)) {
-      KRR_CUDA(cudaStreamSynchronize(c->h2d_stream));  // no copy may still read the caller's Y0
-      return fail(KRR_ERR_INVALID, "Y0 must be finite");
-    }
+    if (!all_finite_parallel(host_Y0, (size_t)total * 8)) return fail(KRR_ERR_INVALID, "Y0 must be finite");
     d_Y0 = dst;
   }
   Pipeline p;
   int rc = prepare_pipeline(c->device, images, (int)ims.size(), total, d_Y0, launch, d_out, d_work, work_size, p);
-  if (rc) {
-    KRR_CUDA(cudaStreamSynchronize(c->h2d_stream));
-    return rc;
-  }
+  if (rc) return rc;
   krr::Queue* qs[4] = {p.w.q0, p.w.q1, p.w.q2, p.w.q3};
   krr::Queue init[4];
   std::memset(init, 0, sizeof(init));
