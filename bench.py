@@ -284,6 +284,32 @@ def best_plain(K, specs, local: int, stream, flush, steps: int):
     return sw, best, blk, {str(b): round(t, 3) for b, t in by_block.items()}
 
 
+def escape_surface_errors(K, specs, a, b) -> dict:
+    """Terminal directions of two traces of the same images compared where each ray that
+    escaped in both crosses the escape surface (their final states are the first accepted
+    steps beyond it, which depend on the step sequence): |d theta| and |d phi| in rad."""
+    import torch
+
+    dth, dph = [], []
+    for k, spec in enumerate(specs):
+        lo, hi = int(a.offsets[k]), int(a.offsets[k + 1])
+        r_esc = float(spec.term.escape_radius)
+        ya, sa = a.tensors["Y"][lo:hi], a.tensors["state"][lo:hi]
+        yb, sb = b.tensors["Y"][lo:hi], b.tensors["state"][lo:hi]
+        tha, pha = K.escape_directions(spec.spacetime, ya, sa, r_esc)
+        thb, phb = K.escape_directions(spec.spacetime, yb, sb, r_esc)
+        both = (sa == 1) & (sb == 1)
+        dth.append((tha - thb).abs()[both])
+        dph.append(torch.remainder(pha - phb + math.pi, 2 * math.pi).sub(math.pi).abs()[both])
+    out = {}
+    for name, v in (("dtheta", torch.cat(dth)), ("dphi", torch.cat(dph))):
+        v = v.double()
+        out[name] = {"median": float(v.median()), "p99": float(torch.quantile(v[:10_000_000], 0.99)),
+                     "max": float(v.max())}
+    out["rays"] = int(sum(x.numel() for x in dth))
+    return out
+
+
 def edge_rms_px(K, spec, state: np.ndarray) -> float:
     """rms distance (px) of the captured-mask edge from Bardeen's curve after the finite-distance
     correction (``raytracing/boundary.py``: 1/8-px marching of the bilinear 0.5 level set)."""
@@ -453,6 +479,7 @@ def run_ours(args) -> None:
         extra["persistent_rays_s"] = total / (kernel_ms * 1e-3)
         extra["speedup_persistent_vs_plain"] = t_plain / kernel_ms
         extra["mask_identical_persistent_vs_plain"] = bool(torch.equal(plain.tensors["state"], sweep.tensors["state"]))
+        extra["escape_surface_vs_plain"] = escape_surface_errors(K, specs, sweep, plain)
         plain.close()
         del plain
         torch.cuda.empty_cache()
