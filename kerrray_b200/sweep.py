@@ -181,6 +181,14 @@ class SweepResult:
     def state_image(self, k: int) -> np.ndarray:
         return self.arrays["state"][self.rows(k)].reshape(self.specs[k].camera.shape)
 
+    def shadow_image(self, k: int):
+        """Image ``k`` as a :class:`~kerrray_b200.shadow.ShadowImage` (``.save(path)`` writes the
+        reference's ``.npz``, format version 1; ``shadow.py:119-176``)."""
+        from kerrray_b200.shadow import _image_from_result
+
+        spec = self.specs[k]
+        return _image_from_result(spec.spacetime, spec.camera, self.result(k))
+
     def captured(self, k: int) -> np.ndarray:
         return self.state_image(k) == int(TerminationState.CAPTURED)
 
@@ -297,6 +305,27 @@ class DeviceSweep:
         _lib.check(_lib.lib().krr_plan_stats(self.plan, torch.cuda.current_stream(self.device).cuda_stream,
                                              ctypes.byref(st)))
         return st.as_dict()
+
+    def result(self, k: int) -> BatchResult:
+        """Image ``k``'s rows of the device results, copied to host arrays."""
+        names = ("n_steps", "n_rejected", "lam", "max_null_error", "max_energy_drift", "max_lz_drift",
+                 "max_carter_drift")
+        if any(n not in self.tensors for n in names):
+            raise ValueError("a minimal sweep keeps only Y and state; build it with minimal=False")
+        lo, hi = int(self.offsets[k]), int(self.offsets[k + 1])
+        host = {n: t[lo:hi].cpu().numpy() for n, t in self.tensors.items()}
+        return BatchResult(Y=host["Y"], state=host["state"], n_steps=host["n_steps"], n_rejected=host["n_rejected"],
+                           lam=host["lam"], max_null_error=host["max_null_error"],
+                           max_energy_drift=host["max_energy_drift"], max_lz_drift=host["max_lz_drift"],
+                           max_carter_drift=host["max_carter_drift"], runtime_s=0.0)
+
+    def shadow_image(self, k: int):
+        """Image ``k`` from the device buffers as a :class:`~kerrray_b200.shadow.ShadowImage`
+        (``.save(path)`` writes the reference's ``.npz``, format version 1)."""
+        from kerrray_b200.shadow import _image_from_result
+
+        spec = self.specs[k]
+        return _image_from_result(spec.spacetime, spec.camera, self.result(k))
 
     def close(self) -> None:
         if self.plan is not None:

@@ -161,3 +161,28 @@ def test_shadow_npz_round_trip(tmp_path: Path) -> None:
     assert back.camera == cam
     mask = K.shadow_mask_int8(img.state)
     assert mask.dtype == np.int8 and int((mask == 1).sum()) == 1250
+
+
+def test_batched_trace_writes_the_reference_npz(tmp_path: Path) -> None:
+    """Image k of a batched trace (SweepResult rows) as the reference's ShadowImage file."""
+    from kerrray_b200.sweep import SweepResult
+
+    d = golden("shadow64_a0.9_i60")
+    st = K.Spacetime(1.0, 0.9)
+    small = K.ImageSpec(st, K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=2),
+                        K.IntegratorOptions(), K.TerminationOptions())
+    big = K.ImageSpec(st, K.Camera(radius=1000.0, inclination_deg=60.0, fov=8.0, resolution=64),
+                      K.IntegratorOptions(rtol=1e-6, atol=1e-8), K.TerminationOptions())
+    def rows(key, dtype=None):
+        x = np.asarray(d[key]) if dtype is None else np.asarray(d[key]).astype(dtype)
+        return np.concatenate([x[:4], x])
+    arrays = {"Y": rows("Y"), "state": rows("state", np.int64), "n_steps": rows("n_steps", np.int64),
+              "n_rejected": rows("n_rejected", np.int64), "lam": rows("lam"), "max_null_error": rows("max_null_error"),
+              "max_energy_drift": rows("max_energy_drift"), "max_lz_drift": rows("max_lz_drift"),
+              "max_carter_drift": rows("max_carter_drift"), "event_Y": None, "event_hit": None}
+    sw = SweepResult(specs=[small, big], offsets=np.array([0, 4, 4 + 4096]), arrays=arrays, stats={})
+    back = K.ShadowImage.load(sw.shadow_image(1).save(tmp_path / "img1.npz"))
+    assert np.array_equal(back.state.ravel(), np.asarray(d["state"]).astype(np.int64))
+    assert back.camera == big.camera and back.count(K.TerminationState.CAPTURED) == 1250
+    assert sw.shadow_image(0).state.shape == (2, 2)
+

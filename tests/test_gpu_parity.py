@@ -480,6 +480,22 @@ def test_bisection_with_more_items_than_lanes_is_the_sequential_bisection() -> N
     assert np.array_equal(r2, r_mid) and np.array_equal(w2, width) and np.array_equal(f2, fails)
 
 
+def test_device_sweep_writes_the_reference_npz(tmp_path) -> None:
+    """A device-resident sweep's image, written from its device buffers as the reference's
+    .npz (format version 1), is the image the drop-in backend's compute_shadow gives."""
+    st = K.Spacetime(1.0, 0.9)
+    specs = [K.ImageSpec(st, K.Camera(radius=1000.0, inclination_deg=i, fov=8.0, resolution=16),
+                         K.IntegratorOptions(rtol=1e-6, atol=1e-8), K.TerminationOptions()) for i in (17.0, 60.0)]
+    dev = K.DeviceSweep(specs, precision="fast64")
+    dev.run()
+    img = K.ShadowImage.load(dev.shadow_image(1).save(tmp_path / "s.npz"))
+    ref = K.compute_shadow(st, specs[1].camera, specs[1].integ, specs[1].term,
+                           backend=K.CudaBackend(precision="fast64"))
+    assert np.array_equal(img.state, ref.state) and np.array_equal(img.result.Y, ref.result.Y)
+    assert img.camera == specs[1].camera
+    dev.close()
+
+
 def test_exact_checks_on_the_cuda_backend() -> None:
     """The reference's Schwarzschild exact checks (configs/schwarzschild.yaml settings: rtol 1e-9,
     atol 1e-11, 15 probes per iteration, brackets [2.5, 4] M and [4, 7] M, tolerance 1e-6 M):
