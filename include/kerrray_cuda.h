@@ -320,6 +320,20 @@ KRR_API int krr_trace_images_noalloc(int device, const krr_image* images, int32_
  * dependent FMA chains timed with CUDA events; the roofline denominator of the step kernels. */
 KRR_API int krr_fma_peak(int device, int fp64, double* tflops);
 
+/* Accretion-disk shading (raytracing/renderer.py:188-199, render_disk's step 3; physics/
+ * redshift.py:131 redshift_factor; physics/accretion.py:180-195 observed_intensity) of n traced rays, device arrays,
+ * enqueued on `stream`: for every row with d_hit[i] != 0, the redshift factor g = nu_obs / nu_em
+ * of the crossing state d_event_Y[i] (n x 8, the stored reversed momentum as the integrator
+ * writes it) for a circular equatorial Keplerian emitter (prograde != 0: a L_z > 0), and
+ * I_obs = g^redshift_power (r / r_in)^-emissivity_index on r_in <= r <= r_out, 0 outside;
+ * d_r_hit = r.  Rows without a hit get g = r_hit = NaN and I = 0.  A hit that is not equatorial
+ * (to 1e-6), lies where no circular orbit exists, or gives g <= 0 gets g = NaN: the reference
+ * raises ValueError there, and so do this library's Python bindings. */
+KRR_API int krr_disk_shading(int device, double mass, double spin, int32_t prograde, double r_in, double r_out,
+                             double emissivity_index, int32_t redshift_power, const double* d_event_Y,
+                             const uint8_t* d_hit, int64_t n, double* d_g, double* d_intensity, double* d_r_hit,
+                             void* stream);
+
 /* Accuracy utility with no counterpart in the reference: the step kernels' own sine and cosine
  * forms at n angles (device arrays), enqueued on `stream`.  which 0: the FP32 sine and cosine of
  * an FP64 angle (reduced by the nearest multiple of pi/2; the mixed mode's accepted states);

@@ -36,6 +36,7 @@ from kerrray_b200.boundary import (
 from kerrray_b200.camera import Camera, initial_states, initial_states_at
 from kerrray_b200.orbits import critical_impact_parameters, shadow_curve
 from kerrray_b200.rays import concatenate_results, trace_rays
+from kerrray_b200.renderer import DiskImage, DiskModel, load_disk_image_arrays, render_disk, save_disk_image
 from kerrray_b200.shadow import FAILURE_STATES, ShadowImage, compute_shadow, shadow_mask_int8, state_counts
 from kerrray_b200.sweep import (
     RETRACE_CRITICAL,
@@ -83,4 +84,5 @@ __all__ = [
     "concatenate_results", "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
     "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
     "RETRACE_CRITICAL", "RETRACE_EDGE", "analytic_classes", "escape_directions", "trig_eval",
+    "DiskImage", "DiskModel", "load_disk_image_arrays", "render_disk", "save_disk_image",
 ]

@@ -28,7 +28,7 @@ EXPORTS = (
     "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
     "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy", "krr_bisect_edges",
     "krr_lensing_workspace_size", "krr_lensing_adjoint", "krr_lensing_replay", "krr_analytic_classes",
-    "krr_escape_directions", "krr_trig_eval",
+    "krr_escape_directions", "krr_trig_eval", "krr_disk_shading",
 )
 
 
@@ -132,6 +132,9 @@ def lib() -> ctypes.CDLL:
         L.krr_workspace_size.argtypes = [i32, i64]
         L.krr_analytic_classes.restype = ctypes.c_int
         L.krr_analytic_classes.argtypes = [dp, dp, dp, dp, vp, i64, vp]
+        L.krr_disk_shading.restype = ctypes.c_int
+        L.krr_disk_shading.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int32, dp, dp, dp, ctypes.c_int32, vp, vp, i64,
+                                       vp, vp, vp, vp]
         L.krr_trig_eval.restype = ctypes.c_int
         L.krr_trig_eval.argtypes = [ctypes.c_int, ctypes.c_int32, vp, vp, i64, vp, vp, vp]
         L.krr_escape_directions.restype = ctypes.c_int

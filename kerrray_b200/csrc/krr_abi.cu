@@ -923,6 +923,25 @@ int krr_integrate_batch(int device, double mass, double spin, const double* Y0, 
   return KRR_OK;
 }
 
+int krr_disk_shading(int device, double mass, double spin, int32_t prograde, double r_in, double r_out,
+                     double emissivity_index, int32_t redshift_power, const double* d_event_Y, const uint8_t* d_hit,
+                     int64_t n, double* d_g, double* d_intensity, double* d_r_hit, void* stream) {
+  int rc = validate_spacetime(mass, spin);
+  if (rc) return rc;
+  if (!(std::isfinite(r_in) && std::isfinite(r_out) && 0.0 < r_in && r_in < r_out))
+    return fail(KRR_ERR_INVALID, "need 0 < r_in < r_out, got r_in=%g, r_out=%g", r_in, r_out);
+  if (!std::isfinite(emissivity_index)) return fail(KRR_ERR_INVALID, "emissivity_index must be finite");
+  if (redshift_power != 3 && redshift_power != 4)
+    return fail(KRR_ERR_INVALID, "redshift_power must be 3 or 4, got %d", redshift_power);
+  if (n < 0) return fail(KRR_ERR_INVALID, "n must be >= 0");
+  if (n == 0) return KRR_OK;
+  if (!d_event_Y || !d_hit || !d_g || !d_intensity || !d_r_hit) return fail(KRR_ERR_INVALID, "device buffers must not be NULL");
+  KRR_CUDA(cudaSetDevice(device));
+  KRR_CUDA(krr::disk_shading(mass, spin * mass, prograde != 0, r_in, r_out, emissivity_index, redshift_power, d_event_Y,
+                             d_hit, n, d_g, d_intensity, d_r_hit, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
 int krr_trig_eval(int device, int32_t which, const double* d_theta, const double* d_delta, int64_t n, double* d_sin,
                   double* d_cos, void* stream) {
   if (which < 0 || which > 2) return fail(KRR_ERR_INVALID, "which must be 0, 1 or 2, got %d", which);

@@ -168,6 +168,58 @@ cudaError_t trig_eval(int which, const double* theta, const double* delta, long 
   return cudaGetLastError();
 }
 
+// Accretion-disk shading of the disk-plane crossings (raytracing/renderer.py:render_disk step
+// 3): the redshift factor g = nu_obs / nu_em of each crossing state for a circular equatorial
+// Keplerian emitter (physics/redshift.py:redshift_factor, BPT 1972 eq. 2.16 for Omega, u^t from
+// the normalisation at theta = pi/2) and I_obs = g^n (r / r_in)^-p on r_in <= r <= r_out
+// (physics/accretion.py:observed_intensity).  g = (-p_t) / (-p_mu u^mu) is the same for the
+// stored (reversed) momentum.  Rows without a hit: g = r_hit = NaN, I = 0; a hit that is not
+// equatorial (to 1e-6), lies where no circular orbit exists, or gives g <= 0 gets g = NaN (the
+// caller raises, as the reference does).
+__global__ void k_disk_shading(double m, double a, int prograde, double r_in, double r_out, double p_index, int n_pow,
+                               const double* __restrict__ Y, const unsigned char* __restrict__ hit, long long n,
+                               double* __restrict__ g_out, double* __restrict__ i_out, double* __restrict__ r_hit) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double g = CUDART_NAN, inten = 0.0, rh = CUDART_NAN;
+  if (hit[i]) {
+    const double* y = Y + 8 * i;
+    const double r = y[1], th = y[2], pt = y[4], pph = y[7];
+    rh = r;
+    const double s = prograde ? 1.0 : -1.0;
+    const double sa = (a < 0.0) ? -1.0 : 1.0;
+    const double sqm = sqrt(m);
+    const double om = s * sa * sqm / (r * sqrt(r) + s * fabs(a) * sqm);
+    const double g_tt = -(1.0 - 2.0 * m / r);
+    const double g_tph = -2.0 * m * a / r;
+    const double g_phph = r * r + a * a + 2.0 * m * a * a / r;
+    const double rad = -(g_tt + 2.0 * om * g_tph + om * om * g_phph);
+    if (fabs(th - 0.5 * CUDART_PI) <= 1e-6 && isfinite(rad) && rad > 0.0) {
+      const double ut = 1.0 / sqrt(rad);
+      const double gg = pt / (pt * ut + pph * (om * ut));
+      if (isfinite(gg) && gg > 0.0) {
+        g = gg;
+        double gn = gg * gg * gg;
+        if (n_pow == 4) gn *= gg;
+        if (r >= r_in && r <= r_out) inten = pow(r / r_in, -p_index) * gn;
+      }
+    }
+  }
+  g_out[i] = g;
+  i_out[i] = inten;
+  r_hit[i] = rh;
+}
+
+cudaError_t disk_shading(double m, double a, int prograde, double r_in, double r_out, double p_index, int n_pow,
+                         const double* Y, const unsigned char* hit, long long n, double* g, double* inten, double* r_hit,
+                         cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int block = 256;
+  k_disk_shading<<<(unsigned)((n + block - 1) / block), block, 0, s>>>(m, a, prograde, r_in, r_out, p_index, n_pow, Y,
+                                                                       hit, n, g, inten, r_hit);
+  return cudaGetLastError();
+}
+
 // Count of the non-finite values among n doubles (added to *count).
 __global__ void k_count_nonfinite(const double* __restrict__ x, long long n, unsigned long long* count) {
   unsigned long long mine = 0;

@@ -23,6 +23,11 @@ const Variant* mixed_sat_variant();
 cudaError_t escape_directions(const Params& P, double r_s, const double* Y, const long long* state, long long n,
                               double* theta, double* phi, cudaStream_t s);
 
+// Disk shading of n crossing states (see k_disk_shading): g, I_obs and r of each hit row.
+cudaError_t disk_shading(double m, double a, int prograde, double r_in, double r_out, double p_index, int n_pow,
+                         const double* Y, const unsigned char* hit, long long n, double* g, double* inten, double* r_hit,
+                         cudaStream_t s);
+
 // Adds to *count (device) the number of non-finite values among the n doubles at x (device).
 cudaError_t count_nonfinite(const double* x, long long n, unsigned long long* count, int sms, cudaStream_t s);
 
