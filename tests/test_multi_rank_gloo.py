@@ -93,3 +93,16 @@ def test_shards_are_disjoint_and_balanced() -> None:
     assert shard.shard_specs(specs[:1], 0, 2) == [0] and shard.shard_specs(specs[:1], 1, 2) == []
     with pytest.raises(ValueError):
         shard.shard_specs(specs, 2, 2)
+
+
+def test_single_process_gather_and_reduce() -> None:
+    """Without a process group the helpers are the identity; a missing image is an error."""
+    assert shard.max_over_ranks(3.5) == 3.5
+    assert shard.gather_results([1, 0], ["b", "a"], 2) == ["a", "b"]
+    with pytest.raises(RuntimeError):
+        shard.gather_results([0], ["a"], 2)
+    with pytest.raises(ValueError):
+        shard.gather_results([0, 1], ["a"], 2)
+    with pytest.raises(ValueError):
+        shard.replicate_specs(_specs(), 0)
+
