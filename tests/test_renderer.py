@@ -60,6 +60,25 @@ def test_disk_model_and_shading_formula_match_the_reference() -> None:
         K.DiskModel.for_spacetime(st, r_in=1.5)
 
 
+def test_oracle_crossings_are_the_reference_crossings() -> None:
+    """The oracle (the reference's kernel restated in C++) on the renderer's camera rays with the
+    disk-plane event reproduces the reference's crossing states bit for bit."""
+    from oracle import oracle as O
+
+    d = golden("render_disk24")
+    m, spin = float(d["mass"]), float(d["spin"])
+    a, b = O.pixel_coordinates(float(d["camera_fov"]), int(d["camera_resolution"]))
+    y0 = O.initial_states(m, spin, float(d["camera_radius"]), float(d["camera_inclination_deg"]), 0.0, a, b)
+    for tag in ("pro", "retro"):
+        opts = O.Options(rtol=float(d["rtol"]), atol=float(d["atol"]), disk_plane=True, r_in=float(d[f"{tag}_r_in"]),
+                         r_out=float(d[f"{tag}_r_out"]))
+        out = O.integrate(m, spin, y0, opts, threads=4)
+        hit = d[f"{tag}_hit"].ravel()
+        assert np.array_equal(out["state"], d[f"{tag}_state"].ravel())
+        assert np.array_equal(out["event_hit"].astype(bool), hit)
+        assert np.array_equal(out["event_Y"][hit], d[f"{tag}_hit_states"].reshape(-1, 8)[hit])
+
+
 @pytest.mark.gpu
 def test_render_disk_matches_the_reference(tmp_path) -> None:
     d = golden("render_disk24")
