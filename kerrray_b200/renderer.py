@@ -19,7 +19,7 @@ import numpy as np
 
 from kerrray_b200 import _lib
 from kerrray_b200.camera import Camera, initial_states
-from kerrray_b200.orbits import equatorial_photon_orbit_radius
+from kerrray_b200.orbits import _mass_and_spin, equatorial_photon_orbit_radius
 from kerrray_b200.types import BatchResult, EventOptions, TerminationState
 
 __all__ = ["DiskModel", "DiskImage", "INTENSITY_LAWS", "isco_radius", "keplerian_angular_velocity", "event_options",
@@ -27,11 +27,6 @@ __all__ = ["DiskModel", "DiskImage", "INTENSITY_LAWS", "isco_radius", "keplerian
 
 INTENSITY_LAWS = {"g3": 3, "g4": 4}  # power of g multiplying the emitted intensity
 STATE_SIZE = 8
-
-
-def _mass_and_spin(st: Any) -> tuple[float, float]:
-    mass = float(st.mass)
-    return mass, float(st.spin) * mass
 
 
 def keplerian_angular_velocity(st: Any, r, prograde: bool = True):
