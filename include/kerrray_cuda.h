@@ -300,16 +300,17 @@ KRR_API int krr_lensing_replay(int device, const krr_lens_params* params, const 
 
 /* Allocation-free form of krr_trace_images_device.  No counterpart in the reference.  For
  * callers that cannot allocate device memory on this path (an application that owns a fixed
- * device-memory budget, work enqueued on a stream another library captures, a plug-in whose
- * host owns all device memory): the launch's scratch (work-queue counters and image
- * descriptors) lives in a static array in the library's device image, sized for at most
- * KRR_NOALLOC_MAX_IMAGES images (about 46 KB per device, held until exit); larger batches are
- * rejected with KRR_ERR_INVALID.  Inputs (d_Y0, nullable) and outputs (d_out) are the caller's
- * device buffers; nothing is allocated.  The first call on a device looks up the array's
- * device address, so make that first call before any stream capture.  All calls share the
- * one array (its counters are cleared at the start of each call): calls that overlap on the
- * GPU race, so serialise them (one stream, or one call at a time).  Synchronises `stream`;
- * kernel_ms is reported as 0. */
+ * device-memory budget and forbids allocations after start-up, a plug-in whose host owns all
+ * device memory): the launch's scratch (work-queue counters and image descriptors) lives in a
+ * static array in the library's device image, sized for at most KRR_NOALLOC_MAX_IMAGES images
+ * (about 46 KB per device, held until exit); larger batches are rejected with KRR_ERR_INVALID.
+ * Inputs (d_Y0, nullable) and outputs (d_out) are the caller's device buffers; nothing is
+ * allocated.  The first call on a device looks up the array's device address.  All calls share
+ * the one array (its counters, and the disk-event outputs when given, are cleared at the start
+ * of each call): calls that overlap on the GPU race, so serialise them (one stream, or one call
+ * at a time).  The call is synchronous: it uploads the descriptors from host memory, reads the
+ * counters back and synchronises `stream`, so it must not run during a stream capture (a
+ * capturing stream is refused with KRR_ERR_UNSUPPORTED).  kernel_ms is reported as 0. */
 #define KRR_NOALLOC_MAX_IMAGES 128
 KRR_API int krr_trace_images_noalloc(int device, const krr_image* images, int32_t n_images, const double* d_Y0,
                                      const krr_launch* launch, const krr_result* d_out, void* stream,

@@ -3,13 +3,16 @@
 //
 // Some callers must not call cudaMalloc or any allocating routine on the path they run: a
 // host application with its own device-memory pool (a renderer or a serving process that
-// budgets every byte up front and forbids allocations after start-up), code that runs on a
-// stream another library captures, or a plug-in whose host framework owns all device memory.
-// This entry point takes the caller's inputs and outputs and keeps the launch's scratch -- the
-// work-queue counters and the image descriptors -- in a fixed array in this library's device
-// image, so it allocates nothing.  The array is sized for KRR_NOALLOC_MAX_IMAGES images; every
-// GPU that loads the library holds it (the queue plus 128 descriptors of 360 B: about 46 KB) until
-// the process exits.
+// budgets every byte up front and forbids allocations after start-up), or a plug-in whose host
+// framework owns all device memory.  This entry point takes the caller's inputs and outputs and
+// keeps the launch's scratch -- the work-queue counters and the image descriptors -- in a fixed
+// array in this library's device image, so it allocates nothing.  The array is sized for
+// KRR_NOALLOC_MAX_IMAGES images; every GPU that loads the library holds it (the queue plus 128
+// descriptors of 360 B: about 46 KB) until the process exits.
+//
+// The call is synchronous: it uploads the descriptors from a host stack buffer, reads the
+// counters back and synchronises the stream.  It therefore cannot run inside a stream capture,
+// and refuses a stream that is capturing.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -89,15 +92,22 @@ extern "C" int krr_trace_images_noalloc(int device, const krr_image* images, int
   const int idx = (launch && launch->variant > 0) ? launch->variant : 0;
   if (!vs || idx >= count) return fail(KRR_ERR_INVALID, "launch variant %d out of range [0, %d)", idx, count);
   if (cudaSetDevice(device) != cudaSuccess) return fail(KRR_ERR_NO_DEVICE, "cannot select device %d", device);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &capturing) != cudaSuccess || capturing != cudaStreamCaptureStatusNone)
+    return fail(KRR_ERR_UNSUPPORTED, "krr_trace_images_noalloc synchronises its stream and cannot run during a stream capture");
   void* scratch = nullptr;
   rc = scratch_address(device, &scratch);
   if (rc) return rc;
-  const cudaStream_t s = static_cast<cudaStream_t>(stream);
   krr::Queue* d_q = static_cast<krr::Queue*>(scratch);
   krr::Image* d_images = reinterpret_cast<krr::Image*>(static_cast<unsigned char*>(scratch) + kQueueBytes);
   cudaError_t e = cudaMemcpyAsync(d_images, ims, (size_t)n_images * sizeof(krr::Image), cudaMemcpyHostToDevice, s);
   // The counters keep the previous call's values: clear them before every launch.
   if (e == cudaSuccess) e = cudaMemsetAsync(d_q, 0, sizeof(krr::Queue), s);
+  // The kernel writes the disk-event outputs only for rays that hit the disk: clear them first,
+  // as the workspace entry point does.
+  if (e == cudaSuccess && d_out->event_Y) e = cudaMemsetAsync(d_out->event_Y, 0, (size_t)total * 8 * sizeof(double), s);
+  if (e == cudaSuccess && d_out->event_hit) e = cudaMemsetAsync(d_out->event_hit, 0, (size_t)total, s);
   if (e != cudaSuccess) return fail(KRR_ERR_CUDA, "scratch upload: %s", cudaGetErrorString(e));
   const int occ = vs[idx].occupancy();
   if (occ < 1) return fail(KRR_ERR_CUDA, "persistent kernel variant %d cannot be resident", idx);
@@ -119,16 +129,13 @@ extern "C" int krr_trace_images_noalloc(int device, const krr_image* images, int
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(KRR_ERR_CUDA, "persistent kernel: %s", cudaGetErrorString(e));
   if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
     stats->photons = (uint64_t)total;
     stats->retired = q.retired;
     stats->attempts = q.attempts;
     stats->accepted = q.accepted;
     stats->lane_slots = q.lane_iters;
     stats->busy_slots = q.busy_iters;
-    stats->kernel_ms = 0.0;
-    stats->retraced = 0;
-    stats->retrace_attempts = 0;
-    stats->retrace_ms = 0.0;
   }
   if (q.error) return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
   if (q.retired != (unsigned long long)total)

@@ -1,9 +1,10 @@
 """Generate the golden fixtures of the per-ray hot path from the KerrRay reference.
 
-Run in a container where the reference source tree is present (it is read,
-never modified)::
+Run where the reference source tree is present (it is read, never modified):
+by default the ``reference`` directory beside this repository's root, or the
+tree that ``KRR_REFERENCE`` names::
 
-    KRR_REFERENCE=/root/reference python tests/golden/make_golden.py
+    KRR_REFERENCE=<reference tree> python tests/golden/make_golden.py
 
 Every fixture is produced by the reference's own code: its ``numba`` backend
 (``src/kerrray/raytracing/backends/numba_backend.py:131-207``, the FP64 oracle
@@ -25,7 +26,7 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("KRR_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("KRR_REFERENCE") or Path(__file__).resolve().parents[3] / "reference")
 OUT = Path(__file__).resolve().parent
 
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/krr_numba_cache")
