@@ -311,19 +311,9 @@ def escape_surface_errors(K, specs, a, b) -> dict:
 
 
 def edge_rms_px(K, spec, state: np.ndarray) -> float:
-    """rms distance (px) of the captured-mask edge from Bardeen's curve after the finite-distance
-    correction (``raytracing/boundary.py``: 1/8-px marching of the bilinear 0.5 level set)."""
-    from kerrray_b200.boundary import mask_centroid
-
-    cam = spec.camera
-    captured = state.reshape(cam.shape) == 2
-    alpha, beta = cam.pixel_coordinates()
-    c = mask_centroid(alpha, beta, captured)
-    edge = K.extract_boundary_from_mask(alpha, beta, captured, centre=c)
-    curve = K.analytic_boundary(spec.spacetime, cam.inclination_deg, 720)
-    err = K.boundary_error(edge, curve, c, pixel_size=cam.pixel_size,
-                           scale=K.finite_distance_scale(spec.spacetime, cam.radius))
-    return float(err["rms_px"])
+    """rms distance (px) of the captured-mask edge (the bilinear interpolant's 0.5 level set)
+    from Bardeen's exact curve after the finite-distance correction."""
+    return float(K.mask_edge_error(spec.spacetime, spec.camera, state == 2)["rms_px"])
 
 
 def sweep_edge_errors(K, specs, state: np.ndarray, offsets) -> dict:

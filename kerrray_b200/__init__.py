@@ -29,13 +29,13 @@ from kerrray_b200.boundary import (
     boundary_error,
     extract_boundary_from_mask,
     finite_distance_scale,
+    mask_edge_error,
     polygon_centroid,
     polygon_radii,
-    summarise_shadow,
 )
 from kerrray_b200.camera import Camera, initial_states, initial_states_at
-from kerrray_b200.orbits import critical_impact_parameters, shadow_curve
-from kerrray_b200.rays import concatenate_results, trace_rays
+from kerrray_b200.orbits import BardeenCurve, critical_impact_parameters, shadow_curve
+from kerrray_b200.rays import trace_rays
 from kerrray_b200.renderer import DiskImage, DiskModel, load_disk_image_arrays, render_disk, save_disk_image
 from kerrray_b200.shadow import FAILURE_STATES, ShadowImage, compute_shadow, shadow_mask_int8, state_counts
 from kerrray_b200.sweep import (
@@ -77,11 +77,11 @@ __all__ = [
     "winding_rate_prediction", "winding_rates",
     "EdgeCase", "analytic_boundary", "bisect_edge", "bisect_edges", "boundary_error", "critical_impact_parameters",
     "edge_options", "edge_study", "extract_boundary_from_mask", "finite_distance_scale", "polygon_centroid",
-    "polygon_radii", "shadow_curve", "summarise_shadow",
+    "polygon_radii", "shadow_curve", "mask_edge_error", "BardeenCurve",
     "BACKEND_NAMES", "Backend", "BackendUnavailable", "BatchResult", "Camera", "CudaBackend", "DeviceSweep",
     "EventOptions", "FAILURE_STATES", "ImageSpec", "IntegratorOptions", "LaunchConfig", "ShadowImage", "Spacetime",
     "SweepResult", "TerminationOptions", "TerminationState", "autotune", "available_backends", "compute_shadow",
-    "concatenate_results", "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
+    "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
     "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
     "RETRACE_CRITICAL", "RETRACE_EDGE", "analytic_classes", "escape_directions", "trig_eval",
     "DiskImage", "DiskModel", "load_disk_image_arrays", "render_disk", "save_disk_image",

@@ -1,73 +1,80 @@
-"""Chunked tracing over any backend (``src/kerrray/raytracing/rays.py:31-117``).
+"""Tracing a batch of initial states on any backend, range by range.
 
-The ``cuda`` backend holds a whole image in device memory, so its default chunk is the whole
-batch; ``chunk_size`` keeps the reference's meaning (and its progress callback) for callers
-that want it.
+The ``cuda`` backend takes the whole batch in one call: the device holds it, and its host-buffer
+path already overlaps the copies of consecutive photon ranges with the trace. Other backends
+(KerrRay's ``numpy`` and ``numba`` objects) are called on consecutive ranges of ``chunk_size``
+rows, and ``progress`` is told the fraction done after each. Every range's per-ray fields are
+written into one result allocated after the first range returns (each array field at the
+batch's length, with that range's dtype), so no list of partial results is kept and joined.
+
+The reference's counterpart is ``raytracing/rays.py:72-117`` (``trace_rays``: 16,384-row
+chunks joined with ``np.concatenate``); the argument meanings and the ``ValueError`` cases are
+the same.
 """
 
 from __future__ import annotations
 
+import dataclasses
 import time
 from typing import Any, Callable
 
 import numpy as np
-from numpy.typing import ArrayLike, NDArray
+from numpy.typing import ArrayLike
 
-from kerrray_b200.backends import get_backend
+from kerrray_b200.backends import CudaBackend, get_backend
 from kerrray_b200.types import STATE_SIZE, BatchResult
 
-__all__ = ["DEFAULT_CHUNK_SIZE", "ProgressCallback", "concatenate_results", "trace_rays"]
+__all__ = ["DEFAULT_CHUNK_SIZE", "HOST_CHUNK_SIZE", "ProgressCallback", "trace_rays"]
 
-DEFAULT_CHUNK_SIZE = 1 << 24
 ProgressCallback = Callable[[float], None]
+DEFAULT_CHUNK_SIZE: int | None = None  # the whole batch on the cuda backend, HOST_CHUNK_SIZE elsewhere
+HOST_CHUNK_SIZE = 1 << 14
 
 
-def _optional_concat(parts: list[NDArray | None]) -> NDArray | None:
-    if any(part is None for part in parts):
-        return None
-    return np.concatenate([part for part in parts if part is not None], axis=0)
-
-
-def concatenate_results(parts: list[Any], runtime_s: float | None = None) -> BatchResult:
-    """Join the per-ray fields of ``parts`` in order into one ``BatchResult``."""
-    if not parts:
-        raise ValueError("concatenate_results needs at least one BatchResult")
-    if len(parts) == 1 and runtime_s is None:
-        return parts[0]
-    cls = type(parts[0])
-    return cls(
-        Y=np.concatenate([p.Y for p in parts], axis=0),
-        state=np.concatenate([p.state for p in parts]),
-        n_steps=np.concatenate([p.n_steps for p in parts]),
-        lam=np.concatenate([p.lam for p in parts]),
-        max_null_error=np.concatenate([p.max_null_error for p in parts]),
-        max_energy_drift=np.concatenate([p.max_energy_drift for p in parts]),
-        max_lz_drift=np.concatenate([p.max_lz_drift for p in parts]),
-        max_carter_drift=np.concatenate([p.max_carter_drift for p in parts]),
-        runtime_s=float(sum(p.runtime_s for p in parts)) if runtime_s is None else float(runtime_s),
-        event_Y=_optional_concat([p.event_Y for p in parts]),
-        event_hit=_optional_concat([p.event_hit for p in parts]),
-        n_rejected=_optional_concat([p.n_rejected for p in parts]),
-    )
+def _per_ray_fields(part: Any, rows: int) -> list[str]:
+    """Names of the array fields of a result that hold one entry per ray."""
+    names = [f.name for f in dataclasses.fields(part)] if dataclasses.is_dataclass(part) else list(vars(part))
+    return [n for n in names if isinstance(getattr(part, n), np.ndarray) and getattr(part, n).shape[:1] == (rows,)]
 
 
 def trace_rays(st: Any, Y0: ArrayLike, integ: Any, term: Any, *, backend: Any = "cuda", events: Any = None,
-               progress: ProgressCallback | None = None, chunk_size: int = DEFAULT_CHUNK_SIZE) -> BatchResult:
-    """Integrate the states ``Y0`` (N, 8), ``N >= 1``, in chunks on ``backend``."""
+               progress: ProgressCallback | None = None, chunk_size: int | None = DEFAULT_CHUNK_SIZE) -> BatchResult:
+    """Integrate the states ``Y0`` (N x 8, N >= 1) on ``backend`` (a name or a backend object)
+    and return one result over all rows, ``runtime_s`` the wall time of the whole call."""
     y0 = np.asarray(Y0)
     if y0.ndim != 2 or y0.shape[1] != STATE_SIZE:
         raise ValueError(f"Y0 must have shape (N, {STATE_SIZE}), got {y0.shape}")
-    n_rays = y0.shape[0]
-    if n_rays < 1:
+    n = int(y0.shape[0])
+    if n < 1:
         raise ValueError("Y0 must contain at least one ray")
-    if chunk_size < 1:
+    if chunk_size is not None and chunk_size < 1:
         raise ValueError(f"chunk_size must be >= 1, got {chunk_size!r}")
     engine = get_backend(backend) if isinstance(backend, str) else backend
-    t0 = time.perf_counter()
-    parts = []
-    for start in range(0, n_rays, chunk_size):
-        stop = min(start + chunk_size, n_rays)
-        parts.append(engine.integrate_batch(st, y0[start:stop], integ, term, events=events))
+    span = chunk_size or (n if isinstance(engine, CudaBackend) else HOST_CHUNK_SIZE)
+    started = time.perf_counter()
+    merged: dict[str, np.ndarray | None] = {}
+    first = None
+    for lo in range(0, n, span):
+        hi = min(lo + span, n)
+        part = engine.integrate_batch(st, y0[lo:hi], integ, term, events=events)
+        if first is None:
+            first = part
+            if hi == n:  # a single range: its result is the batch's
+                break
+            merged = {name: np.empty((n,) + getattr(part, name).shape[1:], getattr(part, name).dtype)
+                      for name in _per_ray_fields(part, hi - lo)}
+        for name, out in merged.items():
+            value = getattr(part, name, None)
+            if out is not None and value is not None:
+                out[lo:hi] = value
+            else:
+                merged[name] = None  # a field that some range does not report is not reported
         if progress is not None:
-            progress(stop / n_rays)
-    return concatenate_results(parts, runtime_s=time.perf_counter() - t0)
+            progress(hi / n)
+    assert first is not None
+    elapsed = time.perf_counter() - started
+    if not merged:
+        if progress is not None:
+            progress(1.0)
+        return dataclasses.replace(first, runtime_s=elapsed)
+    return dataclasses.replace(first, runtime_s=elapsed, **merged)

@@ -184,10 +184,10 @@ class SweepResult:
     def shadow_image(self, k: int):
         """Image ``k`` as a :class:`~kerrray_b200.shadow.ShadowImage` (``.save(path)`` writes the
         reference's ``.npz``, format version 1; ``shadow.py:119-176``)."""
-        from kerrray_b200.shadow import _image_from_result
+        from kerrray_b200.shadow import ShadowImage
 
         spec = self.specs[k]
-        return _image_from_result(spec.spacetime, spec.camera, self.result(k))
+        return ShadowImage.from_result(spec.spacetime, spec.camera, self.result(k))
 
     def captured(self, k: int) -> np.ndarray:
         return self.state_image(k) == int(TerminationState.CAPTURED)
@@ -322,10 +322,10 @@ class DeviceSweep:
     def shadow_image(self, k: int):
         """Image ``k`` from the device buffers as a :class:`~kerrray_b200.shadow.ShadowImage`
         (``.save(path)`` writes the reference's ``.npz``, format version 1)."""
-        from kerrray_b200.shadow import _image_from_result
+        from kerrray_b200.shadow import ShadowImage
 
         spec = self.specs[k]
-        return _image_from_result(spec.spacetime, spec.camera, self.result(k))
+        return ShadowImage.from_result(spec.spacetime, spec.camera, self.result(k))
 
     def close(self) -> None:
         if self.plan is not None:

@@ -151,9 +151,9 @@ def test_shadow_npz_round_trip(tmp_path: Path) -> None:
                         lam=d["lam"], max_null_error=d["max_null_error"], max_energy_drift=d["max_energy_drift"],
                         max_lz_drift=d["max_lz_drift"], max_carter_drift=d["max_carter_drift"], runtime_s=0.1,
                         n_rejected=d["n_rejected"].astype(np.int64))
-    from kerrray_b200.shadow import _image_from_result
+    from kerrray_b200.shadow import ShadowImage
 
-    img = _image_from_result(K.Spacetime(1.0, 0.9), cam, res)
+    img = ShadowImage.from_result(K.Spacetime(1.0, 0.9), cam, res)
     assert img.count(K.TerminationState.CAPTURED) == 1250 and img.n_failed == 0 and img.n_other == 0
     path = img.save(tmp_path / "s.npz")
     back = K.ShadowImage.load(path)
