@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define KRR_ABI_VERSION 3
+#define KRR_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define KRR_API __attribute__((visibility("default")))
@@ -118,11 +118,16 @@ typedef struct krr_camera {
   int64_t resolution;      /* even, >= 2 */
 } krr_camera;
 
-/* One image of a batched launch. */
+/* One image of a batched launch, or a range of its pixels: with pixel_count > 0 the entry
+ * traces pixels first_pixel .. first_pixel + pixel_count - 1 of the camera's grid (row-major),
+ * and its result rows are those pixels in order; pixel_count == 0 (with first_pixel == 0) is the
+ * whole image.  Ranges let several GPUs share one image (KRR_RETRACE_EDGE needs whole images). */
 typedef struct krr_image {
   double mass, spin;
   krr_camera camera;
   krr_options options;
+  int64_t first_pixel;
+  int64_t pixel_count;
 } krr_image;
 
 /* Launch shape of the persistent kernel (0 = library default / autotuned). */
@@ -303,7 +308,7 @@ KRR_API int krr_lensing_replay(int device, const krr_lens_params* params, const 
  * device-memory budget and forbids allocations after start-up, a plug-in whose host owns all
  * device memory): the launch's scratch (work-queue counters and image descriptors) lives in a
  * static array in the library's device image, sized for at most KRR_NOALLOC_MAX_IMAGES images
- * (about 46 KB per device, held until exit); larger batches are rejected with KRR_ERR_INVALID.
+ * (about 47 KB per device, held until exit); larger batches are rejected with KRR_ERR_INVALID.
  * Inputs (d_Y0, nullable) and outputs (d_out) are the caller's device buffers; nothing is
  * allocated.  The first call on a device looks up the array's device address.  All calls share
  * the one array (its counters, and the disk-event outputs when given, are cleared at the start

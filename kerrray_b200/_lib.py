@@ -60,7 +60,8 @@ class KrrCamera(ctypes.Structure):
 
 
 class KrrImage(ctypes.Structure):
-    _fields_ = [("mass", ctypes.c_double), ("spin", ctypes.c_double), ("camera", KrrCamera), ("options", KrrOptions)]
+    _fields_ = [("mass", ctypes.c_double), ("spin", ctypes.c_double), ("camera", KrrCamera), ("options", KrrOptions),
+                ("first_pixel", ctypes.c_int64), ("pixel_count", ctypes.c_int64)]
 
 
 class KrrEdgeCase(ctypes.Structure):

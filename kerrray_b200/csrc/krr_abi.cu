@@ -382,6 +382,24 @@ int copy_rows_back(const krr_result* dev, const krr_result* host, long long r0, 
   return KRR_OK;
 }
 
+// The pixels an image entry covers: [first_pixel, first_pixel + pixel_count) of its grid, or
+// the whole grid when pixel_count is 0.
+int pixel_range(const krr_image& im, long long* first, long long* count) {
+  const long long all = im.camera.resolution * im.camera.resolution;
+  if (im.pixel_count == 0) {
+    if (im.first_pixel != 0) return fail(KRR_ERR_INVALID, "first_pixel must be 0 when pixel_count is 0 (the whole image)");
+    *first = 0;
+    *count = all;
+    return KRR_OK;
+  }
+  if (im.pixel_count < 0 || im.first_pixel < 0 || im.first_pixel > all - im.pixel_count)
+    return fail(KRR_ERR_INVALID, "pixel range [%lld, %lld) lies outside the %lld pixels of the image",
+                (long long)im.first_pixel, (long long)(im.first_pixel + im.pixel_count), all);
+  *first = im.first_pixel;
+  *count = im.pixel_count;
+  return KRR_OK;
+}
+
 // Images -> device descriptors with running offsets.
 int build_images(const krr_image* images, int32_t n_images, std::vector<krr::Image>& out, long long& total) {
   if (!images || n_images < 1) return fail(KRR_ERR_INVALID, "need at least one image");
@@ -397,11 +415,12 @@ int build_images(const krr_image* images, int32_t n_images, std::vector<krr::Ima
     if (rc) return rc;
     rc = validate_grid(&im.camera);
     if (rc) return rc;
+    rc = pixel_range(im, &out[k].first, &out[k].count);
+    if (rc) return rc;
     out[k].P = make_params(im.mass, im.spin, &im.options);
     out[k].fov = im.camera.fov;
     out[k].res = im.camera.resolution;
     out[k].offset = total;
-    out[k].count = im.camera.resolution * im.camera.resolution;
     total += out[k].count;
   }
   // All images of one launch share the scheme and working precision (one kernel instance).
@@ -529,6 +548,11 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     for (int k = 0; k < n_images; ++k)
       if (images[k].options.disk_plane)
         return fail(KRR_ERR_UNSUPPORTED, "the critical-set re-trace classifies ESCAPED/CAPTURED only (no disk events)");
+  }
+  if (p.retrace_mode == KRR_RETRACE_EDGE) {
+    for (int k = 0; k < n_images; ++k)
+      if (images[k].pixel_count != 0)
+        return fail(KRR_ERR_UNSUPPORTED, "the edge re-trace compares every pixel with its 8 neighbours: whole images only");
   }
   const size_t need = work_bytes(n_images, p.retrace ? total : 0);
   if (work_size < need) return fail(KRR_ERR_INVALID, "workspace of %zu bytes is smaller than the %zu needed", work_size, need);

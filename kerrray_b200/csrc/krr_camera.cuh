@@ -30,7 +30,8 @@ struct Image {
   double fov;
   long long res;     // pixels per side
   long long offset;  // first global photon index of this image
-  long long count;   // photons (res * res)
+  long long count;   // photons: its pixels first .. first + count - 1 (row-major)
+  long long first;   // pixel of the image's first photon (0 unless the image is a pixel range)
 };
 
 // (alpha, beta) of pixel p of an n x n image with half-width fov (camera.py:219-222).

@@ -11,6 +11,7 @@ int fail(int code, const char* fmt, ...);
 int validate_options(const krr_options* o);
 int validate_spacetime(double mass, double spin);
 int validate_grid(const krr_camera* c);
+int pixel_range(const krr_image& im, long long* first, long long* count);
 int check_precision(int32_t precision, const krr_options* o);
 krr::Params make_params(double mass, double spin, const krr_options* o);
 int make_frame(double mass, double spin, const krr_camera* c, krr::Frame& F);

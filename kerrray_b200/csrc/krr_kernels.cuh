@@ -56,7 +56,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Initial state of global photon g: a row of Y0, or the camera pixel of its image.
+// Initial state of global photon g: a row of Y0, or the camera pixel of its image (pixel
+// first + (g - offset) of the image's grid).
 __device__ __forceinline__ void photon_source(const Image* __restrict__ images, int img,
                                               const double* __restrict__ Y0, long long g, double y0[8],
                                               Queue* q) {
@@ -65,7 +66,7 @@ __device__ __forceinline__ void photon_source(const Image* __restrict__ images, 
     for (int c = 0; c < 8; ++c) y0[c] = Y0[g * 8 + c];
   } else {
     const Image& im = images[img];
-    if (camera_pixel_state(im, g - im.offset, y0) != 0 && q) atomicCAS(&q->error, 0, 6);
+    if (camera_pixel_state(im, g - im.offset + im.first, y0) != 0 && q) atomicCAS(&q->error, 0, 6);
   }
 }
 

@@ -8,7 +8,7 @@
 // keeps the launch's scratch -- the work-queue counters and the image descriptors -- in a fixed
 // array in this library's device image, so it allocates nothing.  The array is sized for
 // KRR_NOALLOC_MAX_IMAGES images; every GPU that loads the library holds it (the queue plus 128
-// descriptors of 360 B: about 46 KB) until the process exits.
+// descriptors of 368 B: about 47 KB) until the process exits.
 //
 // The call is synchronous: it uploads the descriptors from a host stack buffer, reads the
 // counters back and synchronises the stream.  It therefore cannot run inside a stream capture,
@@ -78,11 +78,12 @@ extern "C" int krr_trace_images_noalloc(int device, const krr_image* images, int
     if (rc) return rc;
     if (im.options.method != images[0].options.method || im.options.dtype != images[0].options.dtype)
       return fail(KRR_ERR_UNSUPPORTED, "all images of one launch must share method and dtype");
+    rc = pixel_range(im, &ims[k].first, &ims[k].count);
+    if (rc) return rc;
     ims[k].P = make_params(im.mass, im.spin, &im.options);
     ims[k].fov = im.camera.fov;
     ims[k].res = im.camera.resolution;
     ims[k].offset = total;
-    ims[k].count = im.camera.resolution * im.camera.resolution;
     total += ims[k].count;
   }
   int rc = check_precision(precision, &images[0].options);

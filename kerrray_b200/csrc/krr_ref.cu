@@ -99,7 +99,7 @@ __global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, 
   if (g < total) {
     const Image& im = images[find_image(images, n_images, g)];
     const long long n = im.res;
-    const long long p = g - im.offset;
+    const long long p = g - im.offset + im.first;  // pixel of the image's grid
     const long long i = p / n, j = p - (p / n) * n;
     const long long s = state[g];
     flag = !(s == ESCAPED || s == CAPTURED);
@@ -107,7 +107,9 @@ __global__ void k_flag_boundary(const Image* __restrict__ images, int n_images, 
       for (int dj = -1; dj <= 1 && !flag; ++dj) {
         const long long ii = i + di, jj = j + dj;
         if ((di == 0 && dj == 0) || ii < 0 || ii >= n || jj < 0 || jj >= n) continue;
-        flag = state[im.offset + ii * n + jj] != s;
+        const long long q = ii * n + jj - im.first;  // the neighbour's row of this launch, if traced in it
+        if (q < 0 || q >= im.count) continue;
+        flag = state[im.offset + q] != s;
       }
     }
   }

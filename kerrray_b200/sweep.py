@@ -90,21 +90,37 @@ def analytic_classes(spacetime, y0: np.ndarray, rtol: float, horizon_epsilon: fl
 
 @dataclass(frozen=True)
 class ImageSpec:
-    """One image of a batched launch."""
+    """One image of a batched launch, or with ``pixels = (first, count)`` the pixels
+    ``first .. first + count - 1`` of its grid (row-major): a share of an image for one GPU."""
 
     spacetime: Any
     camera: Camera
     integ: Any
     term: Any
     events: Any = None
+    pixels: tuple[int, int] | None = None
+
+    def __post_init__(self) -> None:
+        if self.pixels is not None:
+            first, count = (int(x) for x in self.pixels)
+            if count < 1 or first < 0 or first + count > self.camera.n_rays:
+                raise ValueError(f"pixel range {self.pixels} lies outside the image's {self.camera.n_rays} pixels")
+            object.__setattr__(self, "pixels", (first, count))
 
     @property
     def n_rays(self) -> int:
-        return self.camera.n_rays
+        return self.camera.n_rays if self.pixels is None else self.pixels[1]
+
+    @property
+    def whole(self) -> bool:
+        """True when the entry traces every pixel of its image."""
+        return self.pixels is None or self.pixels == (0, self.camera.n_rays)
 
     def as_struct(self) -> _lib.KrrImage:
+        first, count = (0, 0) if self.pixels is None else self.pixels
         return _lib.KrrImage(mass=float(self.spacetime.mass), spin=float(self.spacetime.spin),
-                             camera=self.camera.as_struct(), options=_lib.options_struct(self.integ, self.term, self.events))
+                             camera=self.camera.as_struct(), options=_lib.options_struct(self.integ, self.term, self.events),
+                             first_pixel=first, pixel_count=count)
 
 
 @dataclass(frozen=True)
@@ -179,6 +195,8 @@ class SweepResult:
         )
 
     def state_image(self, k: int) -> np.ndarray:
+        if not self.specs[k].whole:
+            raise ValueError(f"entry {k} is a pixel range, not a whole image")
         return self.arrays["state"][self.rows(k)].reshape(self.specs[k].camera.shape)
 
     def shadow_image(self, k: int):
@@ -187,6 +205,8 @@ class SweepResult:
         from kerrray_b200.shadow import ShadowImage
 
         spec = self.specs[k]
+        if not spec.whole:
+            raise ValueError(f"entry {k} is a pixel range, not a whole image")
         return ShadowImage.from_result(spec.spacetime, spec.camera, self.result(k))
 
     def captured(self, k: int) -> np.ndarray:
@@ -325,6 +345,8 @@ class DeviceSweep:
         from kerrray_b200.shadow import ShadowImage
 
         spec = self.specs[k]
+        if not spec.whole:
+            raise ValueError(f"entry {k} is a pixel range, not a whole image")
         return ShadowImage.from_result(spec.spacetime, spec.camera, self.result(k))
 
     def close(self) -> None:

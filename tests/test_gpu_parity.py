@@ -333,6 +333,30 @@ def test_captured_graph_plan_equals_direct_launch() -> None:
         sw.close()
 
 
+def test_pixel_ranges_of_images_equal_the_whole_images() -> None:
+    """Images cut into pixel ranges (the shares of several GPUs; kerrray_b200.shard) give each
+    pixel exactly the whole image's result, in every precision and with the critical set."""
+    from kerrray_b200 import shard
+
+    specs = _spin99_specs(128)
+    for precision, retrace in (("reference", 0), ("fast64", 0), ("mixed", K.RETRACE_CRITICAL)):
+        cfg = K.LaunchConfig(retrace=retrace)
+        whole = K.trace_images(specs, precision=precision, launch=cfg)
+        for world in (2, 3):
+            for rank in range(world):
+                mine = shard.shard_pieces(specs, rank, world)
+                part = K.trace_images(shard.piece_specs(specs, mine), precision=precision, launch=cfg)
+                assert part.stats["retired"] == sum(p.count for p in mine)
+                for j, p in enumerate(mine):
+                    rows = slice(int(whole.offsets[p.image]) + p.first, int(whole.offsets[p.image]) + p.first + p.count)
+                    for name in ("Y", "state", "n_steps", "n_rejected", "max_null_error"):
+                        assert np.array_equal(part.arrays[name][part.rows(j)], whole.arrays[name][rows]), (precision, name)
+    # the edge re-trace compares neighbours: whole images only
+    piece = shard.piece_specs(specs, [shard.Piece(0, 100, 500)])
+    with pytest.raises(ValueError, match="whole images"):
+        K.trace_images(piece, precision="mixed", launch=K.LaunchConfig(retrace=K.RETRACE_EDGE))
+
+
 def test_plan_creation_waits_for_a_workspace_still_being_filled() -> None:
     """krr_plan_create uploads the image table on its own stream: a workspace whose zero fill is
     still queued on the caller's stream (behind ~50 ms of other work) must not overwrite it."""
