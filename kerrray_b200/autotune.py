@@ -50,17 +50,25 @@ def _signature(specs: Sequence[ImageSpec], precision: str, device: int) -> str:
 
     name = torch.cuda.get_device_name(device)
     rows = sorted({(round(float(s.spacetime.spin), 6), round(float(s.camera.inclination_deg), 4),
-                    int(s.camera.resolution), float(s.integ.rtol), str(s.integ.method)) for s in specs})
+                    int(s.camera.resolution), float(s.integ.rtol), str(s.integ.method),
+                    tuple(s.pixels) if s.pixels is not None else None) for s in specs})
     return json.dumps([name, precision, len(specs), rows])
 
 
 def _reduced(specs: Sequence[ImageSpec], scale: int) -> list[ImageSpec]:
+    """The images at 1/scale of their resolution per side; a pixel range keeps its share of the
+    image (the same fraction of rows at the same place)."""
     out = []
     for s in specs:
         res = max(2, (s.camera.resolution // scale) // 2 * 2)
         cam = Camera(radius=s.camera.radius, inclination_deg=s.camera.inclination_deg, phi_deg=s.camera.phi_deg,
                      fov=s.camera.fov, resolution=res)
-        out.append(replace(s, camera=cam))
+        pixels = None
+        if s.pixels is not None:
+            n, m = s.camera.n_rays, res * res
+            first = s.pixels[0] * m // n
+            pixels = (min(first, m - 1), max(1, min(s.pixels[1] * m // n, m - min(first, m - 1))))
+        out.append(replace(s, camera=cam, pixels=pixels))
     return out
 
 

@@ -1175,7 +1175,7 @@ int krr_plan_destroy(krr_plan* plan) {
 size_t krr_lensing_workspace_size(int64_t n, int32_t tape_capacity, int32_t checkpoint_every) {
   if (n < 0 || tape_capacity < 1 || checkpoint_every < 1) return 0;
   const size_t ck = (size_t)(tape_capacity / checkpoint_every + 1) * 6;
-  return round256((size_t)n * tape_capacity * 8) + round256((size_t)n * ck * 8);
+  return round256((size_t)n * tape_capacity * 8) + round256((size_t)n * ck * 8) + round256((size_t)n * 16 * 8);
 }
 
 static int lens_launch(const krr_lens_params* p, int64_t n, krr::LensLaunch& L, size_t workspace_bytes) {
@@ -1227,6 +1227,9 @@ int krr_lensing_adjoint(int device, const krr_lens_params* params, const double*
   L.status = d_status;
   L.tape_h = static_cast<double*>(workspace);
   L.tape_ck = reinterpret_cast<double*>(static_cast<char*>(workspace) + round256((size_t)n * L.cap * 8));
+  const size_t ck = (size_t)(L.cap / L.K + 1) * 6;
+  L.final_rec = reinterpret_cast<double*>(static_cast<char*>(workspace) + round256((size_t)n * L.cap * 8) +
+                                          round256((size_t)n * ck * 8));
   KRR_CUDA(krr::lensing_adjoint(L, false, static_cast<cudaStream_t>(stream)));
   return KRR_OK;
 }

@@ -20,6 +20,11 @@
 //      derivatives of the 15 metric terms;
 //   5. the chain through the camera Jacobian.
 // Both outputs (theta_e, phi_e) are swept together (two cotangent rows).
+//
+// Steps 1 (its values), 2 and 3 run in k_lensing_forward, which writes each ray's landed final
+// state to the workspace; steps 1 (its Jacobian), 4 and 5 in k_lensing_reverse. Two kernels
+// instead of one keep each within the instruction cache and give each its own register budget:
+// the forward pass is the fast64 step loop, the reverse sweep holds the stage cotangents.
 #include <cuda_runtime.h>
 
 #include "krr_device.cuh"
@@ -116,7 +121,10 @@ struct LensArgs {
   int* status;  // 0 ok, 1 tape full, 2 ended neither ESCAPED nor CAPTURED
   double* tape_h;   // (n, cap)
   double* tape_ck;  // (n, cap / K + 1, NV)
+  double* final_rec;  // (n, FINAL_REC): the landed final state y, f = f(y), p_t, p_phi
 };
+
+constexpr int FINAL_REC = 16;  // y[NV], f[NV], p_t, p_phi, two unused
 
 __device__ __forceinline__ double surface_radius(const Params& P, int state) {
   return state == ESCAPED ? P.r_escape : P.r_capture;
@@ -168,19 +176,14 @@ __device__ void land_on_surface(const Params& P, Ray<Fast64>& ry, const double y
   h_last = h;
 }
 
-__global__ void __launch_bounds__(128) k_lensing_adjoint(LensArgs A) {
+// Forward pass: camera, the integration with the reference controller recording the tape,
+// the landing on the termination surface, the map's value, and the landed final state.
+__global__ void __launch_bounds__(128, 3) k_lensing_forward(LensArgs A) {
   const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n) return;
   const Params& P = A.P;
-  const double m = A.mass, a = A.P.a;
-  // 1. camera and its Jacobian in (alpha, beta, a, theta_o)
-  Dual<4> y0d[8];
-  camera_state_t<Dual<4>>(Dual<4>::var(A.alpha[ray], 0), Dual<4>::var(A.beta[ray], 1), Dual<4>::var(a, 2),
-                          Dual<4>::var(A.th_o, 3), A.r_o, A.ph_o, m, y0d);
   double y0[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) y0[i] = y0d[i].v;
-  // 2. forward pass with the controller; record step sizes and checkpoints
+  camera_state_t<double>(A.alpha[ray], A.beta[ray], A.P.a, A.th_o, A.r_o, A.ph_o, A.mass, y0);
   double* tape_h = A.tape_h + ray * (long long)A.cap;
   const int n_ck = A.cap / A.K + 1;
   double* tape_ck = A.tape_ck + ray * (long long)n_ck * NV;
@@ -217,19 +220,54 @@ __global__ void __launch_bounds__(128) k_lensing_adjoint(LensArgs A) {
   if (status == 0 && ry.state != ESCAPED && ry.state != CAPTURED) status = 2;
   const double rs = surface_radius(P, ry.state);
   if (status == 0 && N > 0) land_on_surface(P, ry, y_prev, rs, tape_h[N - 1]);
-  // 3. the output at the termination surface and its cotangents
-
+  // 3. the output at the termination surface (event-time correction)
   const double dr = ry.y[CR] - rs;
   const double fr = ry.f[CR];
   A.theta[ray] = ry.y[CTH] - ry.f[CTH] / fr * dr;
   A.phi[ray] = ry.y[CPH] - ry.f[CPH] / fr * dr;
+  A.status[ray] = status;
+  double* rec = A.final_rec + ray * FINAL_REC;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    rec[i] = ry.y[i];
+    rec[NV + i] = ry.f[i];
+  }
+  rec[2 * NV] = ry.pt;
+  rec[2 * NV + 1] = ry.pph;
+}
+
+// Reverse pass: the cotangents of the landed output, the checkpointed reverse sweep over the
+// recorded steps, and the chain through the camera's Jacobian.
+__global__ void __launch_bounds__(128) k_lensing_reverse(LensArgs A) {
+  const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (ray >= A.n) return;
   double* J = A.jac + ray * 8;
-  if (status != 0) {
-    A.status[ray] = status;
+  if (A.status[ray] != 0) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) J[i] = CUDART_NAN;
     return;
   }
+  const Params& P = A.P;
+  const double m = A.mass, a = A.P.a;
+  const int N = (int)A.n_steps[ray];
+  const int state = (int)A.state[ray];
+  const double rs = surface_radius(P, state);
+  const double* tape_h = A.tape_h + ray * (long long)A.cap;
+  const int n_ck = A.cap / A.K + 1;
+  const double* tape_ck = A.tape_ck + ray * (long long)n_ck * NV;
+  const double* rec = A.final_rec + ray * FINAL_REC;
+  double yN[NV], fN[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    yN[i] = rec[i];
+    fN[i] = rec[NV + i];
+  }
+  Ray<Fast64> ry{};  // carries the constants p_t, p_phi into the recomputed steps
+  ry.pt = rec[2 * NV];
+  ry.pph = rec[2 * NV + 1];
+  // 3'. the cotangents of the output x_e = x_N - (f_x / f_r)(r_N - r_s)
+  const double dr = yN[CR] - rs;
+  const double fr = fN[CR];
   const int out_comp[NC] = {CTH, CPH};
   double xbar[NC][NX];
   double abar[NC] = {0.0, 0.0};
@@ -241,17 +279,17 @@ __global__ void __launch_bounds__(128) k_lensing_adjoint(LensArgs A) {
       for (int i = 0; i < NX; ++i) xbar[c][i] = 0.0;
 #pragma unroll
       for (int i = 0; i < NV; ++i) v[c][i] = 0.0;
-      const double fx = ry.f[out_comp[c]];
+      const double fx = fN[out_comp[c]];
       xbar[c][out_comp[c]] = 1.0;
       xbar[c][CR] -= fx / fr;
       v[c][out_comp[c]] = -dr / fr;
       v[c][CR] = dr * fx / (fr * fr);
     }
-    rhs_vjp(m, a, ry.y[CR], ry.y[CTH], ry.pt, ry.y[CPR], ry.y[CPTH], ry.pph, v, xbar, abar);
-    if (ry.state == CAPTURED) {  // r_s = r_plus(a) + epsilon moves with a
+    rhs_vjp(m, a, yN[CR], yN[CTH], ry.pt, yN[CPR], yN[CPTH], ry.pph, v, xbar, abar);
+    if (state == CAPTURED) {  // r_s = r_plus(a) + epsilon moves with a
       const double drp_da = -a / sqrt(m * m - a * a);
 #pragma unroll
-      for (int c = 0; c < NC; ++c) abar[c] += ry.f[out_comp[c]] / fr * drp_da;
+      for (int c = 0; c < NC; ++c) abar[c] += fN[out_comp[c]] / fr * drp_da;
     }
   }
   // 4. reverse sweep, segment by segment from the last
@@ -324,6 +362,10 @@ __global__ void __launch_bounds__(128) k_lensing_adjoint(LensArgs A) {
       }
     }
   }
+  // 1'. the camera state's Jacobian in (alpha, beta, a, theta_o) by dual numbers
+  Dual<4> y0d[8];
+  camera_state_t<Dual<4>>(Dual<4>::var(A.alpha[ray], 0), Dual<4>::var(A.beta[ray], 1), Dual<4>::var(a, 2),
+                          Dual<4>::var(A.th_o, 3), A.r_o, A.ph_o, m, y0d);
   // 5. chain through the camera: d/d(alpha, beta, a, theta_o), then a = spin * M
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
@@ -341,8 +383,8 @@ __global__ void __launch_bounds__(128) k_lensing_adjoint(LensArgs A) {
     J[c * 4 + 2] = g[2] * m;
     J[c * 4 + 3] = g[3];
   }
-  A.status[ray] = 0;
 }
+
 
 // Replay: the same camera and the recorded step sequence without the controller (the map the
 // adjoint differentiates), for finite-difference checks.
@@ -390,12 +432,17 @@ cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s) {
   A.status = L.status;
   A.tape_h = L.tape_h;
   A.tape_ck = L.tape_ck;
+  A.final_rec = L.final_rec;
   const int block = 128;
   const unsigned grid = (unsigned)((L.n + block - 1) / block);
-  if (replay)
+  if (replay) {
     k_lensing_replay<<<grid, block, 0, s>>>(A);
-  else
-    k_lensing_adjoint<<<grid, block, 0, s>>>(A);
+    return cudaGetLastError();
+  }
+  k_lensing_forward<<<grid, block, 0, s>>>(A);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_lensing_reverse<<<grid, block, 0, s>>>(A);
   return cudaGetLastError();
 }
 

@@ -57,6 +57,7 @@ struct LensLaunch {
   int* status;
   double* tape_h;
   double* tape_ck;
+  double* final_rec;  // (n, 16) landed final states, written by the forward kernel
 };
 cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s);
 
