@@ -78,7 +78,11 @@ class CudaBackend:
             float32 mode when ``integ.dtype == "float32"``), ``"fast64"`` (FP64 with FMA,
             sincos and Newton reciprocals good to 2^-40 relative; for rtol below about 1e-11
             use ``"reference"``) or ``"mixed"`` (FP32 stages with FP64 accumulation, Delta and
-            error norm; rk45 only).
+            error norm; rk45 only). In the mixed precision the four conservation maxima of the
+            result (``max_null_error`` and the E, L_z and Q drifts) are evaluated in FP32 from
+            the FP32 copy of each accepted state: they bound that copy's round-off (about 1e-7
+            relative), not the drift of the FP64 integration, which ``"fast64"`` and
+            ``"reference"`` report.
 
     Raises:
         BackendUnavailable: When the library, the driver or the device is missing.

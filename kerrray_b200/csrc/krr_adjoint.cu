@@ -15,9 +15,8 @@
 //      step's length);
 //   4. the reverse sweep over the recorded step sequence with the controller held fixed: each
 //      K-step segment is recomputed from its checkpoint, then the adjoint of each DP5 step runs
-//      back through its six stages; the right-hand side's vector-Jacobian product uses the
-//      closed-form momentum derivatives and forward-mode duals for the (r, theta, a)
-//      derivatives of the 15 metric terms;
+//      back through its six stages; the right-hand side's vector-Jacobian product is the
+//      hand-written reverse-mode derivative of the separated right-hand side the steps evaluate;
 //   5. the chain through the camera Jacobian.
 // Both outputs (theta_e, phi_e) are swept together (two cotangent rows).
 //
@@ -41,53 +40,121 @@ constexpr int NX = NV + 2;  // adjoint state: the six integrated components, p_t
 constexpr int XPT = NV, XPPH = NV + 1;
 
 // d(v . f)/d(state, a) at (r, theta, p_t, p_r, p_theta, p_phi) for NC cotangents v (each over
-// the six integrated components of f); accumulates into xbar and abar.  Out of line: the
-// reverse sweep calls it seven times per step, and one copy of its dual-number metric terms
-// instead of seven keeps the kernel within the instruction cache (41 % of the adjoint's time).
+// the six integrated components of f); accumulates into xbar and abar.  f is the right-hand
+// side in Carter's separated form, the one the forward steps evaluate (Fast64::rhs_sc):
+//   Delta = r^2 - 2Mr + a^2, Sigma = r^2 + a^2 - a^2 sin^2, K = (r^2 + a^2) E - a L,
+//   v = L / sin - a E sin, B = v^2 - K^2 / Delta + Delta p_r^2 + p_theta^2  (2 H = B / Sigma),
+//   f_t = (a sin v + (r^2 + a^2) K / Delta) / Sigma,  f_r = Delta p_r / Sigma,
+//   f_theta = p_theta / Sigma,  f_phi = (a K / Delta + L / sin^2 - a E) / Sigma,
+//   f_pr = (r B / Sigma - (r - M) p_r^2 - (K / Delta)((K / Delta)(r - M) - 2 E r)) / Sigma,
+//   f_ptheta = cos (v (L / sin^2 + a E) - a^2 sin B / Sigma) / Sigma,
+// with E = -p_t, L = p_phi (1 / sin dropped for L = 0, the axis guard).  The product is taken by
+// reverse-mode differentiation of that evaluation, written out by hand: the forward values once,
+// then each intermediate's adjoint for both cotangent rows.  Out of line: the reverse sweep
+// calls it seven times per step.
 __device__ __noinline__ void rhs_vjp(double m, double a, double r, double th, double pt, double pr, double pth, double pph,
-                        const double v[NC][NV], double xbar[NC][NX], double abar[NC]) {
-  Dual<3> g[15];
-  metric_terms<Dual<3>>(Dual<3>::var(r, 0), Dual<3>::var(th, 1), Dual<3>::var(a, 2), m, g);
-  if (pph == 0.0) {  // the polar-axis guard of the right-hand side
-    g[4] = Dual<3>(0.0);
-    g[9] = Dual<3>(0.0);
-    g[14] = Dual<3>(0.0);
-  }
-  const double pt2 = pt * pt, ptpph = pt * pph, pr2 = pr * pr, pth2 = pth * pth, pph2 = pph * pph;
+                        const double v_[NC][NV], double xbar[NC][NX], double abar[NC]) {
+  double s, c;
+  sincos(th, &s, &c);
+  const double E = -pt, L = pph, ae = a * E;
+  const double dlt = r * r - 2.0 * m * r + a * a, r2a2 = r * r + a * a;
+  const double as = a * s, a2s = a * as;
+  const double K = r2a2 * E - a * L;
+  const double isig = 1.0 / (r2a2 - a2s * s);
+  const double iD = 1.0 / dlt;
+  const double kd = K * iD;
+  const bool axis = L == 0.0;
+  const double is = axis ? 0.0 : 1.0 / s;
+  const double lis = L * is;
+  const double v = lis - ae * s;
+  const double rm = r - m, pr2 = pr * pr;
+  const double B = v * v - K * kd + dlt * pr2 + pth * pth;
+  const double bs = B * isig;
+  const double T1 = as * v + kd * r2a2;
+  const double T2 = a * kd + lis * is - ae;
+  const double T5 = kd * rm - 2.0 * E * r;
+  const double T4 = rm * pr2 + kd * T5;
+  const double T3 = r * bs - T4;
+  const double T7 = lis * is + ae;
+  const double T6 = v * T7 - a2s * bs;
 #pragma unroll
-  for (int c = 0; c < NC; ++c) {
-    const double vt = v[c][CT], vr = v[c][CR], vth = v[c][CTH], vph = v[c][CPH], vpr = v[c][CPR], vpth = v[c][CPTH];
-    double gb[15];
-    gb[0] = vt * pt;
-    gb[1] = vt * pph + vph * pt;
-    gb[2] = vr * pr;
-    gb[3] = vth * pth;
-    gb[4] = vph * pph;
-    gb[5] = -0.5 * vpr * pt2;
-    gb[6] = -vpr * ptpph;
-    gb[7] = -0.5 * vpr * pr2;
-    gb[8] = -0.5 * vpr * pth2;
-    gb[9] = -0.5 * vpr * pph2;
-    gb[10] = -0.5 * vpth * pt2;
-    gb[11] = -vpth * ptpph;
-    gb[12] = -0.5 * vpth * pr2;
-    gb[13] = -0.5 * vpth * pth2;
-    gb[14] = -0.5 * vpth * pph2;
-    double dr = 0.0, dth = 0.0, da = 0.0;
-#pragma unroll
-    for (int j = 0; j < 15; ++j) {
-      dr = fma(gb[j], g[j].d[0], dr);
-      dth = fma(gb[j], g[j].d[1], dth);
-      da = fma(gb[j], g[j].d[2], da);
-    }
-    xbar[c][CR] += dr;
-    xbar[c][CTH] += dth;
-    abar[c] += da;
-    const double g0 = g[0].v, g1 = g[1].v, g2 = g[2].v, g3 = g[3].v, g4 = g[4].v;
-    xbar[c][XPT] += vt * g0 + vph * g1 - vpr * (g[5].v * pt + g[6].v * pph) - vpth * (g[10].v * pt + g[11].v * pph);
-    xbar[c][XPPH] += vt * g1 + vph * g4 - vpr * (g[6].v * pt + g[9].v * pph) - vpth * (g[11].v * pt + g[14].v * pph);
-    xbar[c][CPR] += vr * g2 - (vpr * g[7].v + vpth * g[12].v) * pr;
-    xbar[c][CPTH] += vth * g3 - (vpr * g[8].v + vpth * g[13].v) * pth;
+  for (int q = 0; q < NC; ++q) {
+    const double wt = v_[q][CT], wr = v_[q][CR], wth = v_[q][CTH], wph = v_[q][CPH], wpr = v_[q][CPR],
+                 wpth = v_[q][CPTH];
+    double u_isig = wt * T1 + wr * dlt * pr + wth * pth + wph * T2 + wpr * T3 + wpth * c * T6;
+    const double uT1 = wt * isig, uT2 = wph * isig, uT3 = wpr * isig, uT6 = wpth * isig * c;
+    const double u_c = wpth * isig * T6;
+    double u_as = uT1 * v;
+    double u_v = uT1 * as + uT6 * T7;
+    double u_kd = uT1 * r2a2 + uT2 * a;
+    double u_r2a2 = uT1 * kd;
+    double u_D = wr * pr * isig;
+    double u_pr = wr * dlt * isig;
+    double u_pth = wth * isig;
+    double u_a = uT2 * kd;
+    double u_lis = uT2 * is;
+    double u_is = uT2 * lis;
+    double u_ae = -uT2;
+    double u_r = uT3 * bs;
+    double u_bs = uT3 * r;
+    const double uT4 = -uT3;
+    double u_rm = uT4 * pr2;
+    double u_pr2 = uT4 * rm;
+    u_kd += uT4 * T5;
+    const double uT5 = uT4 * kd;
+    u_kd += uT5 * rm;
+    u_rm += uT5 * kd;
+    double u_E = -2.0 * r * uT5;
+    u_r -= 2.0 * E * uT5;
+    const double uT7 = uT6 * v;
+    double u_a2s = -uT6 * bs;
+    u_bs -= uT6 * a2s;
+    u_lis += uT7 * is;
+    u_is += uT7 * lis;
+    u_ae += uT7;
+    const double u_B = u_bs * isig;
+    u_isig += u_bs * B;
+    u_v += 2.0 * v * u_B;
+    double u_K = -u_B * kd;
+    u_kd -= u_B * K;
+    u_D += u_B * pr2;
+    u_pr2 += u_B * dlt;
+    u_pth += 2.0 * pth * u_B;
+    u_pr += 2.0 * pr * u_pr2;
+    u_r += u_rm;
+    u_lis += u_v;
+    u_ae -= u_v * s;
+    double u_s = -u_v * ae;
+    double u_L = u_lis * is;
+    u_is += u_lis * L;
+    if (!axis) u_s -= u_is * is * is;
+    u_K += u_kd * iD;
+    u_D -= u_kd * K * iD * iD;
+    const double u_S = -u_isig * isig * isig;
+    u_r2a2 += u_S;
+    u_a2s -= u_S * s;
+    u_s -= u_S * a2s;
+    u_r2a2 += u_K * E;
+    u_E += u_K * r2a2;
+    u_a -= u_K * L;
+    u_L -= u_K * a;
+    u_a += u_a2s * as;
+    u_as += u_a2s * a;
+    u_a += u_as * s;
+    u_s += u_as * a;
+    u_a += u_ae * E;
+    u_E += u_ae * a;
+    u_r += 2.0 * r * u_r2a2;
+    u_a += 2.0 * a * u_r2a2;
+    u_r += 2.0 * rm * u_D;
+    u_a += 2.0 * a * u_D;
+    xbar[q][CR] += u_r;
+    xbar[q][CTH] += u_s * c - u_c * s;
+    xbar[q][CPR] += u_pr;
+    xbar[q][CPTH] += u_pth;
+    xbar[q][XPT] -= u_E;
+    xbar[q][XPPH] += u_L;
+    abar[q] += u_a;
   }
 }
 

@@ -141,7 +141,12 @@ class TerminationState(IntEnum):
 
 @dataclass
 class BatchResult:
-    """Final states and per-ray summaries of a batch (fields and dtypes as the reference)."""
+    """Final states and per-ray summaries of a batch (fields and dtypes as the reference).
+
+    ``max_null_error``, ``max_energy_drift``, ``max_lz_drift`` and ``max_carter_drift`` are the
+    running maxima over accepted steps. From the ``cuda`` backend in its ``"mixed"`` precision
+    they are evaluated in FP32 from the FP32 copy of each accepted state, so they measure that
+    copy's round-off (about 1e-7 relative) rather than the FP64 integration's drift."""
 
     Y: NDArray
     state: NDArray[np.int64]
