@@ -1002,9 +1002,45 @@ def lensing_line(K, args) -> dict:
         walls.append(time.perf_counter() - t0)
     e2e = {"value": n / statistics.mean(walls), "unit": "rays/s", "h2d_bytes_per_step": 2 * 8 * n,
            "d2h_bytes_per_step": (2 + 8) * 8 * n}
+    checks = not getattr(args, "kernel_only", False)
+    fd_check, cpu, fd_vs_oracle, fit, fit_s = None, None, None, None, None
     # FD of the recorded map on a strided sample of >= 8k rays (h = 1e-6); the 20 worst rays
     # again at h = 1e-5 and 1e-7: an error that falls with another h is the FD's, not the adjoint's.
-    idx = torch.arange(0, n, max(1, n // 8192), device=alpha.device)
+    idx = torch.arange(0, n, max(1, n // 8192), device=alpha.device) if checks else None
+    if checks:
+        fd_check, cpu, fd_vs_oracle, fit, fit_s = _lensing_checks(K, A, args, alpha, beta, idx, res, spin, incl, r_o)
+    mag = K.magnification(res.jac)
+    peak64 = _lib.fma_peak_tflops(0, True)
+    roofline = None
+    if LENS_FLOP_PER_STEP is not None:
+        achieved = LENS_FLOP_PER_STEP * total_steps / (kernel_ms * 1e-3) / 1e12
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                    "frac": achieved / peak64, "traffic": None,
+                    "work": f"{LENS_FLOP_PER_STEP} FP64 FLOP per accepted step (the kernels' FP64 instruction "
+                            f"counts from ncu, dfma = 2) x {int(total_steps)} accepted steps",
+                    "peak_source": "measured FP64 FMA chains on this device (krr_fma_peak)"}
+    gn = None if fit is None else {"start": [0.5, 50.0], "target": [spin, incl], "spin": fit["spin"],
+                                   "inclination_deg": fit["inclination_deg"], "iterations": len(fit["history"]) - 1,
+                                   "map_evaluations": fit["evaluations"], "final_cost": fit["history"][-1]["cost"],
+                                   "seconds": fit_s}
+    return _line("lensing-map adjoint rays/s per B200 (forward with tape + reverse sweep, 4 parameters)",
+                 n / (kernel_ms * 1e-3), "rays/s", args, kernel_ms,
+                 {"workload": WORKLOADS["lensing"], "rays": n, "checkpoint_every": 32,
+                  "kernel": "k_lensing_forward + k_lensing_reverse (one ray per thread)",
+                  "l2": "tape of accepted step sizes in HBM (n x 8192 x 8 B), written once and read once"},
+                 e2e=e2e, gpu_launches=2 * args.steps,
+                 roofline=roofline, cpu_baseline=cpu, clocks=clocks.summary(),
+                 rays_ok=ok, accepted_steps={"mean": float(steps.mean().item()), "max": int(steps.max().item()),
+                                             "total": int(total_steps)},
+                 fd_check=fd_check, fd_vs_oracle=fd_vs_oracle, gauss_newton=gn,
+                 magnification={"median": float(mag.median().item()), "max": float(mag.max().item())})
+
+
+def _lensing_checks(K, A, args, alpha, beta, idx, res, spin, incl, r_o):
+    """The lensing line's checks: FD of the recorded map, the CPU baseline with FD of the
+    oracle, and the Gauss-Newton fit."""
+    import torch
+
     sub = A.lensing_map(alpha[idx], beta[idx], spin, incl)
     fd = _fd_replay(A, sub, alpha[idx], beta[idx], spin, incl, 1e-6)
     jac = sub.jac.cpu().numpy()
@@ -1035,31 +1071,7 @@ def lensing_line(K, args) -> dict:
     fit = K.fit_spin_inclination(alpha, beta, res.theta, res.phi, p0=(0.5, 50.0), iterations=20)
     torch.cuda.synchronize()
     fit_s = time.perf_counter() - t0
-    mag = K.magnification(res.jac)
-    peak64 = _lib.fma_peak_tflops(0, True)
-    roofline = None
-    if LENS_FLOP_PER_STEP is not None:
-        achieved = LENS_FLOP_PER_STEP * total_steps / (kernel_ms * 1e-3) / 1e12
-        roofline = {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                    "frac": achieved / peak64, "traffic": None,
-                    "work": f"{LENS_FLOP_PER_STEP} FP64 FLOP per accepted step (the kernel's FP64 instruction "
-                            f"counts from ncu, dfma = 2) x {int(total_steps)} accepted steps",
-                    "peak_source": "measured FP64 FMA chains on this device (krr_fma_peak)"}
-    return _line("lensing-map adjoint rays/s per B200 (forward with tape + reverse sweep, 4 parameters)",
-                 n / (kernel_ms * 1e-3), "rays/s", args, kernel_ms,
-                 {"workload": WORKLOADS["lensing"], "rays": n, "checkpoint_every": 32,
-                  "kernel": "k_lensing_adjoint (one ray per thread)",
-                  "l2": "tape of accepted step sizes in HBM (n x 8192 x 8 B), written once and read once"},
-                 e2e=e2e, gpu_launches=args.steps,
-                 roofline=roofline, cpu_baseline=cpu, clocks=clocks.summary(),
-                 rays_ok=ok, accepted_steps={"mean": float(steps.mean().item()), "max": int(steps.max().item()),
-                                             "total": int(total_steps)},
-                 fd_check=fd_check, fd_vs_oracle=fd_vs_oracle,
-                 gauss_newton={"start": [0.5, 50.0], "target": [spin, incl], "spin": fit["spin"],
-                               "inclination_deg": fit["inclination_deg"], "iterations": len(fit["history"]) - 1,
-                               "map_evaluations": fit["evaluations"],
-                               "final_cost": fit["history"][-1]["cost"], "seconds": fit_s},
-                 magnification={"median": float(mag.median().item()), "max": float(mag.max().item())})
+    return fd_check, cpu, fd_vs_oracle, fit, fit_s
 
 
 def run_lensing(args) -> None:
