@@ -260,15 +260,24 @@ def direction_error(d1: np.ndarray, d2: np.ndarray) -> np.ndarray:
     return np.maximum(dth, dph)
 
 
+# Tolerance scales of the oracle runs that bound its own error at a tolerance: 100x tighter,
+# and 5 % either side.
+ENVELOPE_SCALES = (0.01, 0.95, 1.05)
+
+
 def against_oracle(K, spec, pixels: np.ndarray, gpu_state: np.ndarray, gpu_dirs: np.ndarray, oracle: dict,
                    threads: int | None = None) -> dict:
     """GPU results on ``pixels`` of an image against the oracle's on the same pixels.
 
     Codes must be identical. Terminal states of rays escaped in both are compared on the escape
-    surface; the bar is 10 rtol, or 4x the oracle's own error envelope there (its distance to
-    the oracle at a 100x tighter tolerance, computed for the rays beyond 10 rtol): two valid
-    integrations at one tolerance differ by their global error, which near the photon orbit
-    grows far beyond rtol. Returns the counts and the error distribution in units of rtol."""
+    surface; the bar is 10 rtol, or 4x the oracle's own error envelope there, computed for the
+    rays beyond 10 rtol: the larger of its distance to the oracle at a 100x tighter tolerance
+    and its spread over tolerances 5 % apart (rtol x 0.95 and x 1.05). Two valid integrations at
+    one tolerance differ by their global errors: near the photon orbit these grow far beyond
+    rtol, and a ray whose step sequence takes a few very large steps (the reference's
+    controller has no step cap) has a global error that changes with any change of the sequence
+    -- a tolerance 5 % away, or the FP32 rounding of the mixed stages. Returns the counts and the
+    error distribution in units of rtol."""
     ref_state = np.asarray(oracle["state"], dtype=np.int64)
     differ = np.flatnonzero(ref_state != gpu_state)
     ref_dirs = surface_directions(K, spec, oracle["Y"], ref_state)
@@ -282,11 +291,13 @@ def against_oracle(K, spec, pixels: np.ndarray, gpu_state: np.ndarray, gpu_dirs:
                                       "max": float(err.max()) / rtol},
                     "beyond_10rtol": int(over.size), "beyond_bar": 0})
         if over.size:
-            tight = oracle_pixels(spec, pixels[over], scale=0.01, threads=threads)
-            tight_dirs = surface_directions(K, spec, tight["Y"], tight["state"])
-            env = direction_error(ref_dirs[over], tight_dirs)
-            # A ray that the tighter integration does not see escape lies within the tolerance's
-            # own ambiguity of the shadow edge: its envelope is unbounded.
+            env = np.zeros(over.size)
+            for scale in ENVELOPE_SCALES:
+                other = oracle_pixels(spec, pixels[over], scale=scale, threads=threads)
+                d = direction_error(ref_dirs[over], surface_directions(K, spec, other["Y"], other["state"]))
+                env = np.where(np.isnan(d) | np.isnan(env), np.nan, np.maximum(env, d))
+            # A ray that one of these integrations does not see escape lies within the
+            # tolerance's own ambiguity of the shadow edge: its envelope is unbounded.
             out["envelope_unbounded"] = int((~np.isfinite(env)).sum())
             env = np.where(np.isfinite(env), env, np.inf)
             e_over = err[err > 10 * rtol]

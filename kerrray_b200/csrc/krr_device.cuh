@@ -305,7 +305,14 @@ struct Motion {
 };
 
 // f (six integrated components) at (r, theta, p_r, p_theta) with Delta supplied by the mode.
-template <class T>
+// With T_DEVIATION, f[CT] holds dt/dlambda - E = 2 M r K / (Delta Sigma) instead of dt/dlambda:
+// the identity Sigma dt/dlambda = a sin v + (r^2 + a^2) K / Delta = E Sigma + 2 M r K / Delta.
+// Far from the hole dt/dlambda is E to within 2M/r; an FP32 stage value of it carries rounding
+// noise of 6e-8 E, which the Dormand-Prince error estimate (sum_j E_j k_j, a difference of
+// nearly equal stages) reads as an error of t -- whose scale atol + rtol |t| is small near the
+// observer, where t starts at 0 -- and the controller then takes another step sequence than
+// FP64 would.  The deviation rounds relative to its own, small size instead.
+template <class T, bool T_DEVIATION = false>
 __device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth, const Motion<T>& mo, T a, T a2,
                                               T m, T f[NV]) {
   const T r2a2 = fused(r, r, a2);                          // r^2 + a^2
@@ -320,7 +327,8 @@ __device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth,
   const T rm = r - m;
   const T pr2 = pr * pr;
   const T bs = fused(v, v, fused(-k, kd, fused(dlt, pr2, pth * pth))) * isig;  // 2 H = B / Sigma
-  f[CT] = isig * fused(as, v, kd * r2a2);                  // -dH/dE
+  if constexpr (T_DEVIATION) f[CT] = ((m + m) * r) * kd * isig;  // -dH/dE - E
+  else f[CT] = isig * fused(as, v, kd * r2a2);                      // -dH/dE
   f[CR] = dlt * pr * isig;                                 // dH/dp_r
   f[CTH] = pth * isig;                                     // dH/dp_theta
   f[CPH] = isig * fused(a, kd, fused(lis, is, -mo.ae));    // dH/dL = (a K / Delta + L / sin^2 - a E) / Sigma
@@ -511,10 +519,12 @@ struct Mixed {
     k[2] = make_float2(f[CT], f[CPH]);
   }
 
-  // The right-hand side in FP32 at (r - r_plus = d, r, sin, cos, p_r, p_theta).
+  // The right-hand side in FP32 at (r - r_plus = d, r, sin, cos, p_r, p_theta), its t component
+  // as the deviation dt/dlambda - E (rhs_separated): every stage, the FSAL value ry.f[CT] and
+  // the stage sums of t hold deviations, and the step adds h E to t in FP64.
   __device__ static void rhs_f(const Params& P, float d, float rf, float s, float c, float pr, float pth,
                                const Motion<float>& mo, float f[NV]) {
-    rhs_separated<float>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f);
+    rhs_separated<float, true>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f);
   }
 };
 
@@ -596,7 +606,7 @@ template <class M>
 __device__ __forceinline__ double null_error(const Ray<M>& ry) {
   if constexpr (M::kMixed) {  // FP32, like the stages it checks
     const Motion<float>& mo = ry.sh.mo;
-    float total = -mo.e * ry.f[CT];
+    float total = fmaf(-mo.e, ry.f[CT], -mo.e * mo.e);  // -E (E + deviation)
     total = fmaf(ry.sh.pp.x, ry.f[CR], total);
     total = fmaf(ry.sh.pp.y, ry.f[CTH], total);
     total = fmaf(mo.l, ry.f[CPH], total);
@@ -847,12 +857,13 @@ __device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<M>& r
     es[j] = madd2(es[j], c(dp::E6), kl[j]);
     ha[j] = mul2(h, acc[j]);
   }
-  // The candidate: h * acc rounded in FP32, accumulated into the FP64 state.
+  // The candidate: h * acc rounded in FP32, accumulated into the FP64 state; t adds h E in FP64
+  // beside h times its stages' deviations from E (the weights b sum to 1).
   yn[CR] = ry.y[CR] + (double)ha[0].x;
   yn[CTH] = ry.y[CTH] + (double)ha[0].y;
   yn[CPR] = ry.y[CPR] + (double)ha[1].x;
   yn[CPTH] = ry.y[CPTH] + (double)ha[1].y;
-  yn[CT] = ry.y[CT] + (double)ha[2].x;
+  yn[CT] = ry.y[CT] + fma((double)h, -ry.pt, (double)ha[2].x);
   yn[CPH] = ry.y[CPH] + (double)ha[2].y;
   k6[CR] = kl[0].x;
   k6[CTH] = kl[0].y;
