@@ -713,8 +713,9 @@ def run_ours(args) -> None:
         summary["lensing"] = {"rays_s": lens["value"], "e2e_rays_s": lens["e2e"]["value"],
                               "frac_fp64": (lens["roofline"] or {}).get("frac"),
                               "cpu_rays_s": (lens["cpu_baseline"] or {}).get("value"),
-                              "fd_max_rel": lens["fd_check"]["max_rel"],
-                              "fd_vs_oracle_max_rel": (lens.get("fd_vs_oracle") or {}).get("max_rel"),
+                              "fd_max_rel_h1e-6": lens["fd_check"]["max_rel"],
+                              "fd_worst20_max_rel_best_h": lens["fd_check"]["worst20_max_rel_best_h"],
+                              "fd_vs_oracle_p999_rel": (lens.get("fd_vs_oracle") or {}).get("p999_rel"),
                               "fit": [lens["gauss_newton"]["spin"], lens["gauss_newton"]["inclination_deg"]]}
     if rank == 0:
         chosen = [t for t in tune_report["trials"] if t["variant"] == tuned.variant
@@ -1074,8 +1075,11 @@ def _lensing_checks(K, A, args, alpha, beta, idx, res, spin, incl, r_o):
         ridx = torch.as_tensor(ref["idx"], device=alpha.device)
         jr = A.lensing_map(alpha[ridx], beta[ridx], spin, incl).jac.cpu().numpy()
         e_ref = _fd_error(jr, ref["fd"])
+        per_ray = np.nanmax(e_ref.reshape(e_ref.shape[0], -1), axis=1)
         fd_vs_oracle = {"rays": int(ridx.numel()), "h": 1e-6, "max_rel": float(np.nanmax(e_ref)),
-                        "median_rel": float(np.nanmedian(e_ref)),
+                        "p999_rel": float(np.nanquantile(per_ray, 0.999)), "median_rel": float(np.nanmedian(e_ref)),
+                        "note": "the oracle's controller is live: a ray whose +-h traces take different step "
+                                "sequences has a jump in its FD; the recorded-map check holds the controller fixed",
                         "metric": "|J - FD| / max(|FD|, column RMS), FD of the oracle's adaptive integration, "
                                   "each trace landed on the escape surface"}
     t0 = time.perf_counter()
