@@ -812,21 +812,46 @@ def bisect_line(K, args) -> dict:
     integrate_batch per halving (study_edge_bisection.py:53-68)."""
     from kerrray_b200 import _lib
 
-    cases = bisect_cases(K)
-    n_items = sum(c.angles.size for c in cases)
+    import dataclasses
+
+    from kerrray_b200 import shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    all_cases = bisect_cases(K)
+    # Under torchrun each rank bisects a contiguous run of the (case, direction) items of equal
+    # predicted cost; a direction's bisection depends only on its own history.
+    runs = shard.shard_items([c.rtol ** -0.2 for c in all_cases], [c.angles.size for c in all_cases], rank, world)
+    cases = [dataclasses.replace(all_cases[k], angles=all_cases[k].angles[f:f + n], r_lo=all_cases[k].r_lo[f:f + n],
+                                 r_hi=all_cases[k].r_hi[f:f + n]) for k, f, n in runs]
+    n_items = sum(c.angles.size for c in all_cases)
     iterations = 36
     precision = "reference" if args.precision == "reference" else "fast64"
     for _ in range(args.warmup):
-        K.bisect_edges(cases, 2, precision=precision)
-    with ClockSampler(0) as clocks:
+        K.bisect_edges(cases, 2, precision=precision, device=local)
+    with ClockSampler(local) as clocks:
         kms, walls = [], []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            res, stats = K.bisect_edges(cases, iterations, precision=precision, item_failures=True)
+            res, stats = K.bisect_edges(cases, iterations, precision=precision, item_failures=True, device=local)
             walls.append(time.perf_counter() - t0)
             kms.append(stats["kernel_ms"])
     rays = n_items * iterations
-    kernel_ms = statistics.mean(kms)
+    kernel_ms = shard.max_over_ranks(statistics.mean(kms))
+    wall_s = shard.max_over_ranks(statistics.mean(walls))
+    if world > 1:  # every rank's brackets to every rank, in item order
+        import torch.distributed as dist
+
+        parts = [None] * world
+        dist.all_gather_object(parts, [(k, f, r) for (k, f, _), r in zip(runs, res)])
+        full = [[np.empty(c.angles.size), np.empty(c.angles.size), np.zeros(c.angles.size, np.int64)] for c in all_cases]
+        for part in parts:
+            for k, f, (r_mid, width, fails) in part:
+                for dst, src in zip(full[k], (r_mid, width, fails)):
+                    dst[f:f + src.size] = src
+        res = [tuple(x) for x in full]
+        cases = all_cases
     flops = algorithmic_flops({"attempts": stats["attempts"], "accepted": stats["accepted"], "photons": rays})
     achieved = flops / (kernel_ms * 1e-3) / 1e12
     peak64 = _lib.fma_peak_tflops(0, True)
@@ -855,7 +880,7 @@ def bisect_line(K, args) -> dict:
                    "max_M": float(np.max(v["max_M"])), "rms_over_rtol_median": float(np.median(v["rms_M"])) / float(k),
                    "lost": v["lost"], "lost_directions": v["lost_directions"], "max_width_M": v["max_width_M"],
                    "over": "directions without a lost photon"} for k, v in errors.items()}
-    cpu = None if args.no_cpu else bisect_cpu_baseline(K, cases)
+    cpu = None if (args.no_cpu or world > 1) else bisect_cpu_baseline(K, cases)
     return _line("edge-bisection rays/s per B200 (batched, one persistent launch)", rays / (kernel_ms * 1e-3),
                  "rays/s", args, kernel_ms,
                  {"workload": WORKLOADS["bisect"], "items": n_items, "iterations": iterations, "cases": len(cases),
@@ -863,7 +888,7 @@ def bisect_line(K, args) -> dict:
                             "next midpoints ahead, results bit-identical to sequential bisection)",
                   "curve": "edge error against Bardeen's exact curve (polar radius by bisection on its parameter)",
                   "l2": "inputs < 1 MB; the work is FP64 arithmetic in registers"},
-                 e2e={"value": rays / statistics.mean(walls), "unit": "rays/s", "h2d_bytes_per_step": n_items * 36,
+                 e2e={"value": rays / wall_s, "unit": "rays/s", "h2d_bytes_per_step": n_items * 36,
                       "d2h_bytes_per_step": n_items * 24},
                  gpu_launches=args.steps,
                  roofline={"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
@@ -879,13 +904,39 @@ def bisect_line(K, args) -> dict:
                                 "ahead on the side not taken) are outside the roofline's work"})
 
 
-def run_bisect(args) -> None:
+def _init_ranks():
+    """(rank, world, local): the process group over NCCL under torchrun, nothing otherwise."""
     import torch
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def _finish_ranks(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_bisect(args) -> None:
     import kerrray_b200 as K
 
-    torch.cuda.set_device(0)
-    print(json.dumps(bisect_line(K, args)), flush=True)
+    rank, world, _ = _init_ranks()
+    line = bisect_line(K, args)
+    line["n_gpus"] = world
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    _finish_ranks(world)
 
 
 # FP64 floating-point operations the lensing adjoint kernel executes per accepted step of its
@@ -971,24 +1022,33 @@ def lensing_line(K, args) -> dict:
     from kerrray_b200 import _lib
     from kerrray_b200 import adjoint as A
 
+    from kerrray_b200 import shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
     spin, incl, r_o = 0.8, 60.0, 1000.0
-    alpha, beta = K.edge_distant_rays(spin, incl)
+    alpha, beta = K.edge_distant_rays(spin, incl, device=local)
+    n_job = alpha.numel()
+    # Under torchrun each rank maps a contiguous share of the rays (independent, equal cost).
+    share = shard.split_range(n_job, rank, world)
+    alpha, beta = alpha[share].contiguous(), beta[share].contiguous()
     n = alpha.numel()
-    stream = torch.cuda.current_stream(0)
+    stream = torch.cuda.current_stream(local)
     for _ in range(args.warmup):
-        res = K.lensing_map(alpha, beta, spin, incl)
+        res = K.lensing_map(alpha, beta, spin, incl, device=local)
     torch.cuda.synchronize()
-    with ClockSampler(0) as clocks:
+    with ClockSampler(local) as clocks:
         ms = []
         for _ in range(args.steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            res = K.lensing_map(alpha, beta, spin, incl)
+            res = K.lensing_map(alpha, beta, spin, incl, device=local)
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
-    kernel_ms = statistics.mean(ms)
+    kernel_ms = shard.max_over_ranks(statistics.mean(ms))
     ok = int(((res.status == 0) & (res.state == 1)).sum().item())
     steps = res.n_steps.double()
     total_steps = float(steps.sum().item())
@@ -1004,17 +1064,23 @@ def lensing_line(K, args) -> dict:
     for _ in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        a_d = a_host.to("cuda", non_blocking=True)
-        b_d = b_host.to("cuda", non_blocking=True)
-        r = K.lensing_map(a_d, b_d, spin, incl)
+        a_d = a_host.to(f"cuda:{local}", non_blocking=True)
+        b_d = b_host.to(f"cuda:{local}", non_blocking=True)
+        r = K.lensing_map(a_d, b_d, spin, incl, device=local)
         th_host.copy_(r.theta, non_blocking=True)
         ph_host.copy_(r.phi, non_blocking=True)
         jac_host.copy_(r.jac, non_blocking=True)
         torch.cuda.synchronize()
         walls.append(time.perf_counter() - t0)
-    e2e = {"value": n / statistics.mean(walls), "unit": "rays/s", "h2d_bytes_per_step": 2 * 8 * n,
-           "d2h_bytes_per_step": (2 + 8) * 8 * n}
-    checks = not getattr(args, "kernel_only", False)
+    e2e = {"value": n_job / shard.max_over_ranks(statistics.mean(walls)), "unit": "rays/s",
+           "h2d_bytes_per_step": 2 * 8 * n_job, "d2h_bytes_per_step": (2 + 8) * 8 * n_job}
+    if world > 1:  # every rank's accepted steps (the roofline's work)
+        import torch.distributed as dist
+
+        t = torch.tensor([total_steps], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        total_steps = float(t.item())
+    checks = not getattr(args, "kernel_only", False) and world == 1
     fd_check, cpu, fd_vs_oracle, fit, fit_s = None, None, None, None, None
     # FD of the recorded map on a strided sample of >= 8k rays (h = 1e-6); the 20 worst rays
     # again at h = 1e-5 and 1e-7: an error that falls with another h is the FD's, not the adjoint's.
@@ -1036,8 +1102,8 @@ def lensing_line(K, args) -> dict:
                                    "map_evaluations": fit["evaluations"], "final_cost": fit["history"][-1]["cost"],
                                    "seconds": fit_s}
     return _line("lensing-map adjoint rays/s per B200 (forward with tape + reverse sweep, 4 parameters)",
-                 n / (kernel_ms * 1e-3), "rays/s", args, kernel_ms,
-                 {"workload": WORKLOADS["lensing"], "rays": n, "checkpoint_every": 32,
+                 n_job / (kernel_ms * 1e-3), "rays/s", args, kernel_ms,
+                 {"workload": WORKLOADS["lensing"], "rays": n_job, "rays_per_gpu": n, "checkpoint_every": 32,
                   "kernel": "k_lensing_forward + k_lensing_reverse (one ray per thread)",
                   "l2": "tape of accepted step sizes in HBM (n x 8192 x 8 B), written once and read once"},
                  e2e=e2e, gpu_launches=2 * args.steps,
@@ -1090,12 +1156,14 @@ def _lensing_checks(K, A, args, alpha, beta, idx, res, spin, incl, r_o):
 
 
 def run_lensing(args) -> None:
-    import torch
-
     import kerrray_b200 as K
 
-    torch.cuda.set_device(0)
-    print(json.dumps(lensing_line(K, args)), flush=True)
+    rank, world, _ = _init_ranks()
+    line = lensing_line(K, args)
+    line["n_gpus"] = world
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    _finish_ranks(world)
 
 
 def main() -> None:
