@@ -312,9 +312,16 @@ struct Motion {
 // nearly equal stages) reads as an error of t -- whose scale atol + rtol |t| is small near the
 // observer, where t starts at 0 -- and the controller then takes another step sequence than
 // FP64 would.  The deviation rounds relative to its own, small size instead.
+//
+// With T_DEVIATION and r_deviation (a runtime choice), f[CR] holds dr/dlambda - p_r =
+// p_r (a^2 sin^2 - 2 M r) / Sigma (as Delta = Sigma - 2 M r + a^2 sin^2): far from the hole dr/dlambda
+// is p_r to within 2M/r, and a step's stages then differ from p_r by small amounts that FP32
+// keeps to its relative precision (the r error estimate's rounding noise otherwise steers the
+// controller on long steps, whose r scale rtol r is comparable with 6e-8 h |p_r| / r).  Near the
+// hole, where that difference is most of dr/dlambda, f[CR] is dr/dlambda itself.
 template <class T, bool T_DEVIATION = false>
 __device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth, const Motion<T>& mo, T a, T a2,
-                                              T m, T f[NV]) {
+                                              T m, T f[NV], bool r_deviation = false) {
   const T r2a2 = fused(r, r, a2);                          // r^2 + a^2
   const T as = a * s;
   const T a2s = a * as;                                    // a^2 sin
@@ -329,7 +336,8 @@ __device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth,
   const T bs = fused(v, v, fused(-k, kd, fused(dlt, pr2, pth * pth))) * isig;  // 2 H = B / Sigma
   if constexpr (T_DEVIATION) f[CT] = ((m + m) * r) * kd * isig;  // -dH/dE - E
   else f[CT] = isig * fused(as, v, kd * r2a2);                      // -dH/dE
-  f[CR] = dlt * pr * isig;                                 // dH/dp_r
+  if constexpr (T_DEVIATION) f[CR] = pr * (r_deviation ? fused(a2s, s, -(m + m) * r) : dlt) * isig;
+  else f[CR] = dlt * pr * isig;                            // dH/dp_r
   f[CTH] = pth * isig;                                     // dH/dp_theta
   f[CPH] = isig * fused(a, kd, fused(lis, is, -mo.ae));    // dH/dL = (a K / Delta + L / sin^2 - a E) / Sigma
   // -dH/dr = (r B / Sigma - (r - M) p_r^2 - (K / Delta)((K / Delta)(r - M) - 2 E r)) / Sigma
@@ -471,7 +479,11 @@ struct Mixed {
     float2 rd, pp;
     float th, s0, c0;
     Motion<float> mo;
+    bool far;  // r > FAR_R M: the r stages hold dr/dlambda - p_r (rhs_separated)
   };
+
+  // Radius (in M) beyond which a step carries dr/dlambda as its deviation from the step's p_r.
+  static constexpr double FAR_R = 32.0;
 
   // The accepted state's sine and cosine: the mixed mode needs them only in FP32 (the shadow,
   // the diagnostics), from theta in FP64 (sincos_reduced); the axis test works on theta itself.
@@ -491,13 +503,21 @@ struct Mixed {
     sh.th = (float)y[CTH];
     sh.s0 = (float)tr.s;
     sh.c0 = (float)tr.c;
+    sh.far = y[CR] > FAR_R * P.mass;
+  }
+
+  // After an accepted step: the FSAL value of r in the form of the new state's region (the step
+  // computed it in the form of the old one; they differ only when the step crossed FAR_R).
+  __device__ static void rebase_fsal(bool far_old, const Shadow& sh, K f[NV]) {
+    if (far_old && !sh.far) f[CR] = sh.pp.x + f[CR];
+    else if (!far_old && sh.far) f[CR] = f[CR] - sh.pp.x;
   }
 
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow& sh, K f[NV], Trig& tr) {
     sh.mo.set((float)pt, (float)pph, (float)P.a);
     tr = accept_trig(y[CTH], tr);
     accepted(P, y, sh, tr);
-    rhs_f(P, sh.rd.y, sh.rd.x, sh.s0, sh.c0, sh.pp.x, sh.pp.y, sh.mo, f);
+    rhs_f(P, sh.rd.y, sh.rd.x, sh.s0, sh.c0, sh.pp.x, sh.pp.y, sh.mo, f, sh.far);
   }
 
   // The right-hand side at the stage input shadow + h * acc, from the pairs (r, theta) and
@@ -505,26 +525,34 @@ struct Mixed {
   // Every stage's sine and cosine come from the accepted state's by a small-angle shift; near
   // the axis (|sin| < 1/50, where the shift's sum would cancel) or for a large shift,
   // sincos_reduced of the stage's theta.
-  __device__ static void stage(const Params& P, const Shadow& sh, float h, const float2 acc[2], float2 k[3]) {
+  // node: the stage's c_s (sum of its tableau row).  Far from the hole (sh.far) acc[0].x sums the
+  // stages' deviations of dr/dlambda from the step's p_r, so the r input adds c_s p_r, and the
+  // stage returns its own deviation from that p_r: h sum_j a_sj k_pr,j (its p_r offset) plus
+  // rhs_f's.  dev_r (nullable) receives rhs_f's value alone: the FSAL value of the candidate.
+  __device__ static void stage(const Params& P, const Shadow& sh, float h, float node, const float2 acc[2],
+                               float2 k[3], float* dev_r = nullptr) {
     const float2 hh = make_float2(h, h);
-    const float2 rd = __ffma2_rn(hh, make_float2(acc[0].x, acc[0].x), sh.rd);  // (r, r - r_plus)
-    const float2 pp = __ffma2_rn(hh, acc[1], sh.pp);                           // (p_r, p_theta)
+    const float ar = sh.far ? fmaf(node, sh.pp.x, acc[0].x) : acc[0].x;
+    const float2 rd = __ffma2_rn(hh, make_float2(ar, ar), sh.rd);  // (r, r - r_plus)
+    const float2 pp = __ffma2_rn(hh, acc[1], sh.pp);              // (p_r, p_theta)
     const float dth = h * acc[0].y;
     float s, c;
     if (!(fabsf(sh.s0) >= 0.02f && sincos_shift_x2(sh.s0, sh.c0, dth, s, c))) sincos_reduced((double)(sh.th + dth), s, c);
     float f[NV];
-    rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, f);
-    k[0] = make_float2(f[CR], f[CTH]);
+    rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, f, sh.far);
+    if (dev_r) *dev_r = f[CR];
+    k[0] = make_float2(sh.far ? fmaf(h, acc[1].x, f[CR]) : f[CR], f[CTH]);
     k[1] = make_float2(f[CPR], f[CPTH]);
     k[2] = make_float2(f[CT], f[CPH]);
   }
 
   // The right-hand side in FP32 at (r - r_plus = d, r, sin, cos, p_r, p_theta), its t component
-  // as the deviation dt/dlambda - E (rhs_separated): every stage, the FSAL value ry.f[CT] and
-  // the stage sums of t hold deviations, and the step adds h E to t in FP64.
+  // as the deviation dt/dlambda - E and, with far, its r component as dr/dlambda - p_r
+  // (rhs_separated): every stage, the FSAL values and the stage sums of t (and of r, far from the
+  // hole) hold deviations, and the step adds h E to t (and h p_r to r) in FP64.
   __device__ static void rhs_f(const Params& P, float d, float rf, float s, float c, float pr, float pth,
-                               const Motion<float>& mo, float f[NV]) {
-    rhs_separated<float, true>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f);
+                               const Motion<float>& mo, float f[NV], bool far) {
+    rhs_separated<float, true>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f, far);
   }
 };
 
@@ -596,7 +624,10 @@ __device__ __forceinline__ int classify(const Params& P, const Ray<M>& ry, bool 
   if (r < (S)0.0 || th < (S)(-THETA_TOL) || th > (S)(PI + THETA_TOL)) return OUT_OF_DOMAIN;
   if (ry.pph != (S)0.0 && near_axis<M>(ry)) return OUT_OF_DOMAIN;
   if (r <= (S)P.r_capture) return CAPTURED;
-  if (r >= (S)P.r_escape && ry.f[CR] > (typename M::K)0.0) return ESCAPED;
+  // dr/dlambda = Delta p_r / Sigma has the sign of p_r outside the horizon; the mixed mode's
+  // ry.f[CR] may hold its deviation from p_r, so it reads p_r.
+  const bool outward = M::kMixed ? ry.y[CPR] > (S)0.0 : ry.f[CR] > (typename M::K)0.0;
+  if (r >= (S)P.r_escape && outward) return ESCAPED;
   if (ry.lam >= P.lambda_max || (long long)ry.n_steps >= P.max_steps) return MAX_AFFINE;
   return RUNNING;
 }
@@ -607,7 +638,7 @@ __device__ __forceinline__ double null_error(const Ray<M>& ry) {
   if constexpr (M::kMixed) {  // FP32, like the stages it checks
     const Motion<float>& mo = ry.sh.mo;
     float total = fmaf(-mo.e, ry.f[CT], -mo.e * mo.e);  // -E (E + deviation)
-    total = fmaf(ry.sh.pp.x, ry.f[CR], total);
+    total = fmaf(ry.sh.pp.x, ry.sh.far ? ry.sh.pp.x + ry.f[CR] : ry.f[CR], total);
     total = fmaf(ry.sh.pp.y, ry.f[CTH], total);
     total = fmaf(mo.l, ry.f[CPH], total);
     return (double)fabsf(0.5f * total);
@@ -824,17 +855,17 @@ __device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<M>& r
   k0[2] = make_float2(ry.f[CT], ry.f[CPH]);
 #pragma unroll
   for (int j = 0; j < 2; ++j) acc[j] = mul2(c(dp::A10), k0[j]);
-  Mixed::stage(P, sh, h, acc, k1);
+  Mixed::stage(P, sh, h, 0.2f, acc, k1);
 #pragma unroll
   for (int j = 0; j < 2; ++j) acc[j] = madd2(mul2(c(dp::A20), k0[j]), c(dp::A21), k1[j]);
-  Mixed::stage(P, sh, h, acc, k2);
+  Mixed::stage(P, sh, h, 0.3f, acc, k2);
 #pragma unroll
   for (int j = 0; j < 2; ++j) acc[j] = madd2(madd2(mul2(c(dp::A30), k0[j]), c(dp::A31), k1[j]), c(dp::A32), k2[j]);
-  Mixed::stage(P, sh, h, acc, k3);
+  Mixed::stage(P, sh, h, 0.8f, acc, k3);
 #pragma unroll
   for (int j = 0; j < 2; ++j)
     acc[j] = madd2(madd2(madd2(mul2(c(dp::A40), k0[j]), c(dp::A41), k1[j]), c(dp::A42), k2[j]), c(dp::A43), k3[j]);
-  Mixed::stage(P, sh, h, acc, k4);
+  Mixed::stage(P, sh, h, c(8.0 / 9.0), acc, k4);
 #pragma unroll
   for (int j = 0; j < 2; ++j)
     acc[j] = madd2(madd2(madd2(madd2(mul2(c(dp::A50), k0[j]), c(dp::A51), k1[j]), c(dp::A52), k2[j]), c(dp::A53), k3[j]),
@@ -844,13 +875,14 @@ __device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<M>& r
     bs[j] = madd2(madd2(madd2(mul2(c(dp::B0), k0[j]), c(dp::B2), k2[j]), c(dp::B3), k3[j]), c(dp::B4), k4[j]);
     es[j] = madd2(madd2(madd2(mul2(c(dp::E0), k0[j]), c(dp::E2), k2[j]), c(dp::E3), k3[j]), c(dp::E4), k4[j]);
   }
-  Mixed::stage(P, sh, h, acc, k5);
+  Mixed::stage(P, sh, h, 1.0f, acc, k5);
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     acc[j] = madd2(bs[j], c(dp::B5), k5[j]);
     es[j] = madd2(es[j], c(dp::E5), k5[j]);
   }
-  Mixed::stage(P, sh, h, acc, kl);
+  float dev6;
+  Mixed::stage(P, sh, h, 1.0f, acc, kl, &dev6);
   float2 ha[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
@@ -859,13 +891,13 @@ __device__ __forceinline__ void dp_stages_mixed(const Params& P, const Ray<M>& r
   }
   // The candidate: h * acc rounded in FP32, accumulated into the FP64 state; t adds h E in FP64
   // beside h times its stages' deviations from E (the weights b sum to 1).
-  yn[CR] = ry.y[CR] + (double)ha[0].x;
+  yn[CR] = sh.far ? ry.y[CR] + fma((double)h, ry.y[CPR], (double)ha[0].x) : ry.y[CR] + (double)ha[0].x;
   yn[CTH] = ry.y[CTH] + (double)ha[0].y;
   yn[CPR] = ry.y[CPR] + (double)ha[1].x;
   yn[CPTH] = ry.y[CPTH] + (double)ha[1].y;
   yn[CT] = ry.y[CT] + fma((double)h, -ry.pt, (double)ha[2].x);
   yn[CPH] = ry.y[CPH] + (double)ha[2].y;
-  k6[CR] = kl[0].x;
+  k6[CR] = sh.far ? dev6 : kl[0].x;  // the candidate's deviation from its own p_r, or dr/dlambda
   k6[CTH] = kl[0].y;
   k6[CPR] = kl[1].x;
   k6[CPTH] = kl[1].y;
@@ -994,7 +1026,13 @@ __device__ __forceinline__ void attempt(const Params& P, Ray<M>& ry, double* __r
     ry.f[i] = k6[i];
   }
   ry.tr = M::accept_trig((double)ry.y[CTH], tr);
-  M::accepted(P, ry.y, ry.sh, ry.tr);
+  if constexpr (M::kMixed) {
+    const bool far_old = ry.sh.far;
+    M::accepted(P, ry.y, ry.sh, ry.tr);
+    Mixed::rebase_fsal(far_old, ry.sh, ry.f);
+  } else {
+    M::accepted(P, ry.y, ry.sh, ry.tr);
+  }
   const double lam_old = ry.lam;
   ry.lam = last ? P.lambda_max : ry.lam + (double)h_eff;
   ry.n_steps += 1;
