@@ -477,7 +477,7 @@ struct Mixed {
   // with its sine and cosine, and the ray's constants of motion.
   struct Shadow {
     float2 rd, pp;
-    float th, s0, c0;
+    float ep, psgn, s0, c0;  // theta's distance from the nearer pole (+1: theta, -1: pi - theta)
     Motion<float> mo;
     bool far;  // r > FAR_R M: the r stages hold dr/dlambda - p_r (rhs_separated)
   };
@@ -500,7 +500,9 @@ struct Mixed {
   __device__ static void accepted(const Params& P, const S y[NV], Shadow& sh, const Trig& tr) {
     sh.rd = make_float2((float)y[CR], (float)(y[CR] - P.r_plus));
     sh.pp = make_float2((float)y[CPR], (float)y[CPTH]);
-    sh.th = (float)y[CTH];
+    const bool south = y[CTH] > 0.5 * PI;
+    sh.ep = (float)(south ? PI - y[CTH] : y[CTH]);  // in FP64: FP32 keeps it to its relative precision
+    sh.psgn = south ? -1.0f : 1.0f;
     sh.s0 = (float)tr.s;
     sh.c0 = (float)tr.c;
     sh.far = y[CR] > FAR_R * P.mass;
@@ -524,7 +526,7 @@ struct Mixed {
   // (p_r, p_theta) of acc; k receives f as the pairs (r, theta), (p_r, p_theta), (t, phi).
   // Every stage's sine and cosine come from the accepted state's by a small-angle shift; near
   // the axis (|sin| < 1/50, where the shift's sum would cancel) or for a large shift,
-  // sincos_reduced of the stage's theta.
+  // sincos_reduced of the stage's angle from the nearer pole.
   // node: the stage's c_s (sum of its tableau row).  Far from the hole (sh.far) acc[0].x sums the
   // stages' deviations of dr/dlambda from the step's p_r, so the r input adds c_s p_r, and the
   // stage returns its own deviation from that p_r: h sum_j a_sj k_pr,j (its p_r offset) plus
@@ -537,7 +539,14 @@ struct Mixed {
     const float2 pp = __ffma2_rn(hh, acc[1], sh.pp);              // (p_r, p_theta)
     const float dth = h * acc[0].y;
     float s, c;
-    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift_x2(sh.s0, sh.c0, dth, s, c))) sincos_reduced((double)(sh.th + dth), s, c);
+    if (!(fabsf(sh.s0) >= 0.02f && sincos_shift_x2(sh.s0, sh.c0, dth, s, c))) {
+      // Near the axis (or for a long shift): the sine and cosine of the stage's angle from the
+      // nearer pole, which FP32 holds to its relative precision (theta itself, next to pi, only
+      // to 2.4e-7 absolute: a relative 1e-4 of sin theta at 2e-3 from the axis, which the L/sin
+      // and L/sin^2 terms then carried into the stages).
+      sincos_reduced((double)fmaf(sh.psgn, dth, sh.ep), s, c);
+      c *= sh.psgn;
+    }
     float f[NV];
     rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, f, sh.far);
     if (dev_r) *dev_r = f[CR];
