@@ -939,11 +939,11 @@ def run_bisect(args) -> None:
     _finish_ranks(world)
 
 
-# FP64 floating-point operations the lensing adjoint kernel executes per accepted step of its
-# rays (forward pass, landing, checkpointed reverse sweep and camera chain together), from the
-# kernel's FP64 instruction counts in one ncu capture of this workload (dadd + dmul + 2 dfma
-# thread instructions, divided by the rays' accepted steps). None until measured.
-LENS_FLOP_PER_STEP = None
+# FP64 floating-point operations the two lensing kernels execute per accepted step of their
+# rays (forward pass with landing; checkpointed reverse sweep and camera chain), from their FP64
+# instruction counts in one ncu capture of this workload (dadd + dmul + 2 dfma thread
+# instructions of both launches, divided by the rays' 17,650,736 accepted steps; profiles/).
+LENS_FLOP_PER_STEP = 5161
 
 
 def _fd_error(jac: np.ndarray, fd: np.ndarray) -> np.ndarray:

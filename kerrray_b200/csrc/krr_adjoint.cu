@@ -54,39 +54,41 @@ constexpr int XPT = NV, XPPH = NV + 1;
 // calls it seven times per step.
 __device__ __noinline__ void rhs_vjp(double m, double a, double r, double th, double pt, double pr, double pth, double pph,
                         const double v_[NC][NV], double xbar[NC][NX], double abar[NC]) {
+  // The translation unit rounds every product and sum separately (-fmad=false); the products
+  // accumulated here are fused explicitly (fma), which this derivative needs for no bit pattern.
   double s, c;
   sincos(th, &s, &c);
   const double E = -pt, L = pph, ae = a * E;
-  const double dlt = r * r - 2.0 * m * r + a * a, r2a2 = r * r + a * a;
+  const double dlt = fma(r, r - 2.0 * m, a * a), r2a2 = fma(r, r, a * a);
   const double as = a * s, a2s = a * as;
-  const double K = r2a2 * E - a * L;
-  const double isig = 1.0 / (r2a2 - a2s * s);
+  const double K = fma(r2a2, E, -a * L);
+  const double isig = 1.0 / fma(-a2s, s, r2a2);
   const double iD = 1.0 / dlt;
   const double kd = K * iD;
   const bool axis = L == 0.0;
   const double is = axis ? 0.0 : 1.0 / s;
   const double lis = L * is;
-  const double v = lis - ae * s;
+  const double v = fma(-ae, s, lis);
   const double rm = r - m, pr2 = pr * pr;
-  const double B = v * v - K * kd + dlt * pr2 + pth * pth;
+  const double B = fma(v, v, fma(-K, kd, fma(dlt, pr2, pth * pth)));
   const double bs = B * isig;
-  const double T1 = as * v + kd * r2a2;
-  const double T2 = a * kd + lis * is - ae;
-  const double T5 = kd * rm - 2.0 * E * r;
-  const double T4 = rm * pr2 + kd * T5;
-  const double T3 = r * bs - T4;
-  const double T7 = lis * is + ae;
-  const double T6 = v * T7 - a2s * bs;
+  const double T1 = fma(as, v, kd * r2a2);
+  const double T2 = fma(a, kd, fma(lis, is, -ae));
+  const double T5 = fma(kd, rm, -2.0 * E * r);
+  const double T4 = fma(rm, pr2, kd * T5);
+  const double T3 = fma(r, bs, -T4);
+  const double T7 = fma(lis, is, ae);
+  const double T6 = fma(v, T7, -a2s * bs);
 #pragma unroll
   for (int q = 0; q < NC; ++q) {
     const double wt = v_[q][CT], wr = v_[q][CR], wth = v_[q][CTH], wph = v_[q][CPH], wpr = v_[q][CPR],
                  wpth = v_[q][CPTH];
-    double u_isig = wt * T1 + wr * dlt * pr + wth * pth + wph * T2 + wpr * T3 + wpth * c * T6;
+    double u_isig = fma(wt, T1, fma(wr * dlt, pr, fma(wth, pth, fma(wph, T2, fma(wpr, T3, wpth * c * T6)))));
     const double uT1 = wt * isig, uT2 = wph * isig, uT3 = wpr * isig, uT6 = wpth * isig * c;
     const double u_c = wpth * isig * T6;
     double u_as = uT1 * v;
-    double u_v = uT1 * as + uT6 * T7;
-    double u_kd = uT1 * r2a2 + uT2 * a;
+    double u_v = fma(uT1, as, uT6 * T7);
+    double u_kd = fma(uT1, r2a2, uT2 * a);
     double u_r2a2 = uT1 * kd;
     double u_D = wr * pr * isig;
     double u_pr = wr * dlt * isig;
@@ -100,56 +102,56 @@ __device__ __noinline__ void rhs_vjp(double m, double a, double r, double th, do
     const double uT4 = -uT3;
     double u_rm = uT4 * pr2;
     double u_pr2 = uT4 * rm;
-    u_kd += uT4 * T5;
+    u_kd = fma(uT4, T5, u_kd);
     const double uT5 = uT4 * kd;
-    u_kd += uT5 * rm;
-    u_rm += uT5 * kd;
+    u_kd = fma(uT5, rm, u_kd);
+    u_rm = fma(uT5, kd, u_rm);
     double u_E = -2.0 * r * uT5;
-    u_r -= 2.0 * E * uT5;
+    u_r = fma(-2.0 * E, uT5, u_r);
     const double uT7 = uT6 * v;
     double u_a2s = -uT6 * bs;
-    u_bs -= uT6 * a2s;
-    u_lis += uT7 * is;
-    u_is += uT7 * lis;
+    u_bs = fma(-uT6, a2s, u_bs);
+    u_lis = fma(uT7, is, u_lis);
+    u_is = fma(uT7, lis, u_is);
     u_ae += uT7;
     const double u_B = u_bs * isig;
-    u_isig += u_bs * B;
-    u_v += 2.0 * v * u_B;
+    u_isig = fma(u_bs, B, u_isig);
+    u_v = fma(2.0 * v, u_B, u_v);
     double u_K = -u_B * kd;
-    u_kd -= u_B * K;
-    u_D += u_B * pr2;
-    u_pr2 += u_B * dlt;
-    u_pth += 2.0 * pth * u_B;
-    u_pr += 2.0 * pr * u_pr2;
+    u_kd = fma(-u_B, K, u_kd);
+    u_D = fma(u_B, pr2, u_D);
+    u_pr2 = fma(u_B, dlt, u_pr2);
+    u_pth = fma(2.0 * pth, u_B, u_pth);
+    u_pr = fma(2.0 * pr, u_pr2, u_pr);
     u_r += u_rm;
     u_lis += u_v;
-    u_ae -= u_v * s;
+    u_ae = fma(-u_v, s, u_ae);
     double u_s = -u_v * ae;
     double u_L = u_lis * is;
-    u_is += u_lis * L;
-    if (!axis) u_s -= u_is * is * is;
-    u_K += u_kd * iD;
-    u_D -= u_kd * K * iD * iD;
+    u_is = fma(u_lis, L, u_is);
+    if (!axis) u_s = fma(-u_is * is, is, u_s);
+    u_K = fma(u_kd, iD, u_K);
+    u_D = fma(-u_kd * K, iD * iD, u_D);
     const double u_S = -u_isig * isig * isig;
     u_r2a2 += u_S;
-    u_a2s -= u_S * s;
-    u_s -= u_S * a2s;
-    u_r2a2 += u_K * E;
-    u_E += u_K * r2a2;
-    u_a -= u_K * L;
-    u_L -= u_K * a;
-    u_a += u_a2s * as;
-    u_as += u_a2s * a;
-    u_a += u_as * s;
-    u_s += u_as * a;
-    u_a += u_ae * E;
-    u_E += u_ae * a;
-    u_r += 2.0 * r * u_r2a2;
-    u_a += 2.0 * a * u_r2a2;
-    u_r += 2.0 * rm * u_D;
-    u_a += 2.0 * a * u_D;
+    u_a2s = fma(-u_S, s, u_a2s);
+    u_s = fma(-u_S, a2s, u_s);
+    u_r2a2 = fma(u_K, E, u_r2a2);
+    u_E = fma(u_K, r2a2, u_E);
+    u_a = fma(-u_K, L, u_a);
+    u_L = fma(-u_K, a, u_L);
+    u_a = fma(u_a2s, as, u_a);
+    u_as = fma(u_a2s, a, u_as);
+    u_a = fma(u_as, s, u_a);
+    u_s = fma(u_as, a, u_s);
+    u_a = fma(u_ae, E, u_a);
+    u_E = fma(u_ae, a, u_E);
+    u_r = fma(2.0 * r, u_r2a2, u_r);
+    u_a = fma(2.0 * a, u_r2a2, u_a);
+    u_r = fma(2.0 * rm, u_D, u_r);
+    u_a = fma(2.0 * a, u_D, u_a);
     xbar[q][CR] += u_r;
-    xbar[q][CTH] += u_s * c - u_c * s;
+    xbar[q][CTH] += fma(u_s, c, -u_c * s);
     xbar[q][CPR] += u_pr;
     xbar[q][CPTH] += u_pth;
     xbar[q][XPT] -= u_E;
@@ -305,7 +307,10 @@ __global__ void __launch_bounds__(128, 3) k_lensing_forward(LensArgs A) {
 
 // Reverse pass: the cotangents of the landed output, the checkpointed reverse sweep over the
 // recorded steps, and the chain through the camera's Jacobian.
-__global__ void __launch_bounds__(128) k_lensing_reverse(LensArgs A) {
+#ifndef KRR_LENS_REVERSE_MINB
+#define KRR_LENS_REVERSE_MINB 1  // resident blocks per SM the reverse kernel's registers allow for
+#endif
+__global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(LensArgs A) {
   const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n) return;
   double* J = A.jac + ray * 8;
@@ -388,7 +393,7 @@ __global__ void __launch_bounds__(128) k_lensing_reverse(LensArgs A) {
 #pragma unroll
         for (int j = 0; j < 6; ++j)
 #pragma unroll
-          for (int i = 0; i < NV; ++i) kbar[c][j][i] = h * dp_a(5, j) * xbar[c][i];
+          for (int i = 0; i < NV; ++i) kbar[c][j][i] = (h * dp_a(5, j)) * xbar[c][i];
       for (int s = 5; s >= 1; --s) {  // stage inputs Y_s, s = 5..1, produced k_s
         double v[NC][NV], ybar_s[NC][NX];
 #pragma unroll
@@ -413,7 +418,7 @@ __global__ void __launch_bounds__(128) k_lensing_reverse(LensArgs A) {
             const double w = h * dp_a(sm, j);
             if (w != 0.0) {
 #pragma unroll
-              for (int i = 0; i < NV; ++i) kbar[c][j][i] += w * ybar_s[c][i];
+              for (int i = 0; i < NV; ++i) kbar[c][j][i] = fma(w, ybar_s[c][i], kbar[c][j][i]);
             }
           }
         }
