@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define KRR_ABI_VERSION 4
+#define KRR_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define KRR_API __attribute__((visibility("default")))
@@ -65,9 +65,11 @@ enum {
   KRR_RETRACE_CRITICAL = 2  /* before the trace, each photon's analytic class from its constants of
                                motion (radial potential R(r)); photons within a band of the
                                critical curve run in reference order on SMs of their own, beside
-                               the main trace; afterwards photons whose code is not their analytic
-                               class are traced again in FP64, and what still disagrees (or ended
-                               within 1 % of its affine or step budget) in reference order */
+                               the main trace (and, for a mixed trace, escaping photons within
+                               0.3 M of it in fast FP64 on SMs of their own too); afterwards photons
+                               whose code is not their analytic class are traced again in FP64, and
+                               what still disagrees (or ended within 1 % of its affine or step
+                               budget) in reference order */
 };
 
 /* termination codes (photons/classification.py:60-69) */
@@ -170,6 +172,10 @@ typedef struct krr_stats {
   uint64_t speculative; /* krr_bisect_edges: photons traced ahead of their bracket by idle lanes */
   uint64_t discarded_attempts; /* krr_bisect_edges: attempts of those photons whose side was not
                                   taken (not in `attempts`, which counts the sequential bisection's) */
+  uint64_t near_edge;   /* KRR_RETRACE_CRITICAL with KRR_PREC_MIXED: escaping photons within the
+                           near-edge band of the shadow boundary, traced in fast FP64 beside the
+                           mixed trace (their exit directions need FP64) */
+  uint64_t near_edge_attempts;
 } krr_stats;
 
 KRR_API const char* krr_last_error(void);

@@ -87,7 +87,8 @@ class KrrStats(ctypes.Structure):
                 ("kernel_ms", ctypes.c_double), ("retraced", ctypes.c_uint64), ("retrace_attempts", ctypes.c_uint64),
                 ("retrace_ms", ctypes.c_double), ("critical", ctypes.c_uint64), ("rechecked", ctypes.c_uint64),
                 ("critical_ms", ctypes.c_double), ("speculative", ctypes.c_uint64),
-                ("discarded_attempts", ctypes.c_uint64)]
+                ("discarded_attempts", ctypes.c_uint64), ("near_edge", ctypes.c_uint64),
+                ("near_edge_attempts", ctypes.c_uint64)]
 
     def as_dict(self) -> dict[str, Any]:
         return {name: getattr(self, name) for name, _ in self._fields_}

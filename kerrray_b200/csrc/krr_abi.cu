@@ -466,18 +466,22 @@ struct WorkLayout {
   krr::Queue* q1;
   krr::Queue* q2;
   krr::Queue* q3;
+  krr::Queue* q4;  // the near-edge photons of the critical-set pipeline
   krr::Image* images;
   long long* list;
+  long long* near_list;
   unsigned char* risk;
 };
 
 constexpr size_t round256(size_t x) { return (x + 255) / 256 * 256; }
-constexpr size_t kQueueArea = 1024;  // four queues, 256 bytes apart
+constexpr size_t kQueueArea = 1280;  // five queues, 256 bytes apart
 static_assert(sizeof(krr::Queue) <= 256, "a queue must fit its 256-byte slot of the workspace");
 
+// With re-trace entries: the list, the near-edge list (8 bytes per entry each) and the
+// analytic classes (1 byte).
 size_t work_bytes(int n_images, long long list_entries) {
   const size_t n = (size_t)std::max(list_entries, 0LL);
-  return kQueueArea + round256((size_t)std::max(n_images, 0) * sizeof(krr::Image)) + round256(n * 8) + n;
+  return kQueueArea + round256((size_t)std::max(n_images, 0) * sizeof(krr::Image)) + 2 * round256(n * 8) + n;
 }
 
 WorkLayout work_layout(void* base, int n_images, long long list_entries) {
@@ -487,10 +491,13 @@ WorkLayout work_layout(void* base, int n_images, long long list_entries) {
   w.q1 = reinterpret_cast<krr::Queue*>(b + 256);
   w.q2 = reinterpret_cast<krr::Queue*>(b + 512);
   w.q3 = reinterpret_cast<krr::Queue*>(b + 768);
+  w.q4 = reinterpret_cast<krr::Queue*>(b + 1024);
   const size_t list_at = kQueueArea + round256((size_t)n_images * sizeof(krr::Image));
+  const size_t list_bytes = round256((size_t)std::max(list_entries, 0LL) * 8);
   w.images = reinterpret_cast<krr::Image*>(b + kQueueArea);
   w.list = reinterpret_cast<long long*>(b + list_at);
-  w.risk = reinterpret_cast<unsigned char*>(b + list_at + round256((size_t)std::max(list_entries, 0LL) * 8));
+  w.near_list = reinterpret_cast<long long*>(b + list_at + list_bytes);
+  w.risk = reinterpret_cast<unsigned char*>(b + list_at + 2 * list_bytes);
   return w;
 }
 
@@ -515,6 +522,9 @@ struct Pipeline {
   const krr::Variant* crit_v = nullptr;
   krr::PersistArgs fix{};   // the FP64 re-trace of photons unlike their analytic class
   const krr::Variant* fix_v = nullptr;
+  bool near = false;        // KRR_RETRACE_CRITICAL of a mixed trace: the near-edge photons in fast FP64
+  krr::PersistArgs nearby{};
+  const krr::Variant* near_v = nullptr;
 };
 
 // Registers one resident block of a kernel holds (allocated per warp in units of 256).
@@ -633,6 +643,28 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     p.re.grid = sms * p.re_v->occupancy();
     p.re.block = p.re_v->block;
     p.re.d_total = &p.w.q3->flagged;
+    if (precision == KRR_PREC_MIXED) {
+      // Escaping photons near the shadow edge (krr_radial.cuh:near_band) pass near the
+      // unstable photon orbit, which magnifies the FP32 stages' round-off in their exit
+      // direction: they are traced in fast FP64 by a third kernel, launched after the critical
+      // one in the same way (one block fills an SM, programmatic dependent launch, the next
+      // kernel launching as soon as its blocks run), and the mixed trace skips them.  It
+      // waits for the critical kernel at its exit, so the mixed trace's exit wait covers both.
+      const krr::Variant* nv = krr::near_wide_variant();
+      if (nv->occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "the near-edge kernel cannot be resident");
+      p.near = true;
+      p.near_v = nv;
+      p.nearby = p.crit;
+      p.nearby.q = p.w.q4;
+      p.nearby.grid = std::max(1, std::min(sms - crit_sms - 1, (sms * 12 + 50) / 100));
+      p.nearby.block = nv->block;
+      p.nearby.index = p.w.near_list;
+      p.nearby.d_total = &p.w.q4->flagged;
+      p.nearby.risk = p.w.risk;  // a photon ending near a budget is marked for the re-check
+      p.nearby.flags = krr::TRACE_SPREAD;
+      p.nearby.pdl = krr::PDL_TRIGGER | krr::PDL_WAIT;
+      p.main.flags |= krr::TRACE_SKIP_NEAR;
+    }
   }
   return KRR_OK;
 }
@@ -646,8 +678,10 @@ cudaError_t enqueue_critical(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0,
   if (e == cudaSuccess && ev0) e = cudaEventRecord(ev0, s);
   const long long* state = reinterpret_cast<const long long*>(p.out.state);
   if (e == cudaSuccess)
-    e = krr::risk_prepass(p.w.images, p.n_images, p.total, p.main.Y0, p.w.risk, p.w.list, p.w.q1, s);
+    e = krr::risk_prepass(p.w.images, p.n_images, p.total, p.main.Y0, p.w.risk, p.w.list, p.w.q1,
+                          p.near ? p.w.near_list : nullptr, p.w.q4, s);
   if (e == cudaSuccess) e = p.crit_v->run(p.crit, s);  // critical photons, reference order
+  if (e == cudaSuccess && p.near) e = p.near_v->run(p.nearby, s);  // near-edge photons, fast FP64
   if (e == cudaSuccess) e = p.main_v->run(p.main, s);  // programmatic dependent: runs beside it
   if (e == cudaSuccess && ev1) e = cudaEventRecord(ev1, s);
   if (e == cudaSuccess) e = krr::check_risk(p.w.images, p.n_images, p.total, p.w.risk, state, p.w.list, p.w.q2, false, s);
@@ -691,12 +725,13 @@ cudaError_t enqueue_pipeline(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0,
 // Read the counters back (synchronises the stream) and check the queue's bookkeeping.
 int finish_pipeline(const Pipeline& p, cudaStream_t s, krr_stats* stats, cudaEvent_t ev0, cudaEvent_t ev1,
                     cudaEvent_t ev2) {
-  krr::Queue q[4];
+  krr::Queue q[5];
   std::memset(q, 0, sizeof(q));
   KRR_CUDA(cudaMemcpyAsync(&q[0], p.w.q0, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaMemcpyAsync(&q[1], p.w.q1, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaMemcpyAsync(&q[2], p.w.q2, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaMemcpyAsync(&q[3], p.w.q3, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
+  if (p.near) KRR_CUDA(cudaMemcpyAsync(&q[4], p.w.q4, sizeof(krr::Queue), cudaMemcpyDeviceToHost, s));
   KRR_CUDA(cudaStreamSynchronize(s));
   const bool crit = p.retrace_mode == KRR_RETRACE_CRITICAL;
   float ms = 0.0f, ms2 = 0.0f;
@@ -717,8 +752,10 @@ int finish_pipeline(const Pipeline& p, cudaStream_t s, krr_stats* stats, cudaEve
     stats->critical = crit ? q[1].flagged : 0;
     stats->critical_ms = ms_c;
     stats->rechecked = crit ? q[2].flagged + q[3].flagged : 0;
+    stats->near_edge = p.near ? q[4].flagged : 0;
+    stats->near_edge_attempts = p.near ? q[4].attempts : 0;
   }
-  if (q[0].error || q[1].error || q[2].error || q[3].error)
+  if (q[0].error || q[1].error || q[2].error || q[3].error || q[4].error)
     return fail(KRR_ERR_NOT_NULL, "tetrad projection is not null to 1e-10 (or no null momentum exists)");
   if (q[0].retired != (unsigned long long)p.total)
     return fail(KRR_ERR_CUDA, "work-queue inconsistency: %llu photons retired of %lld", q[0].retired, p.total);
@@ -726,6 +763,8 @@ int finish_pipeline(const Pipeline& p, cudaStream_t s, krr_stats* stats, cudaEve
     return fail(KRR_ERR_CUDA, "critical-set inconsistency: %llu of %llu critical, %llu of %llu and %llu of %llu "
                 "rechecked photons retired", q[1].retired, q[1].flagged, q[2].retired, q[2].flagged, q[3].retired,
                 q[3].flagged);
+  if (p.near && q[4].retired != q[4].flagged)
+    return fail(KRR_ERR_CUDA, "near-edge inconsistency: %llu of %llu photons retired", q[4].retired, q[4].flagged);
   if (p.retrace && !crit && q[1].retired != q[0].flagged)
     return fail(KRR_ERR_CUDA, "re-trace inconsistency: %llu photons retired of %llu flagged", q[1].retired, q[0].flagged);
   return KRR_OK;

@@ -48,6 +48,11 @@ const Variant* fast_variants(bool mixed, bool rk4, int* count) {
   return f64;
 }
 
+const Variant* near_wide_variant() {
+  static const Variant v = make_variant<Fast64, false, 384, 1>();
+  return &v;
+}
+
 // The mixed re-trace of the few rays an FP32 overflow ended early (MixedSat: an overflowing
 // trial step is a rejection, as in FP64).
 const Variant* mixed_sat_variant() {

@@ -140,7 +140,8 @@ __global__ void k_trace_plain(Params P, const Image* __restrict__ images, int n_
 // TRACE_RESUME -- a photon continues from the result row already in the outputs (its last
 // accepted state, affine parameter, counters and drift maxima: a trace that an FP32 overflow
 // ended early) with the first step size, instead of starting again at the camera.
-enum : int { TRACE_SPREAD = 1, TRACE_RESUME = 2 };
+// TRACE_SKIP_NEAR -- RISK_NEAR photons are skipped as well (the near-edge kernel traces them).
+enum : int { TRACE_SPREAD = 1, TRACE_RESUME = 2, TRACE_SKIP_NEAR = 4 };
 
 template <class M>
 __device__ __forceinline__ void resume_from_outputs(const Params& P, const Outputs& o, long long g, Ray<M>& ry) {
@@ -220,8 +221,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
         const unsigned long long mine = base + (unsigned long long)rank;
         if (mine < (unsigned long long)total) {
           g = index ? index[mine] : (long long)mine;
-          if (risk && risk[g] == RISK_CRITICAL) {
-            atomicAdd(&q->retired, 1ull);  // traced by the reference-order kernel
+          if (risk && (risk[g] == RISK_CRITICAL || ((flags & TRACE_SKIP_NEAR) && risk[g] == RISK_NEAR))) {
+            atomicAdd(&q->retired, 1ull);  // traced by the reference-order or the near-edge kernel
           } else {
             img = find_image(images, n_images, g);
             const Image& im = images[img];
@@ -724,10 +725,12 @@ constexpr Variant make_variant() {
 }
 
 // Analytic classes of every photon (krr_radial.cuh) into risk[]; the critical photons'
-// global indices are appended to `list` and counted in q->flagged.
+// global indices are appended to `list` and counted in q->flagged, and with near_list the
+// near-edge photons' to near_list, counted in q_near->flagged.
 __global__ void k_risk_prepass(const Image* __restrict__ images, int n_images, long long total,
                                const double* __restrict__ Y0, unsigned char* __restrict__ risk,
-                               long long* __restrict__ list, Queue* q);
+                               long long* __restrict__ list, Queue* q, long long* __restrict__ near_list,
+                               Queue* q_near);
 
 // After the traces: every non-critical photon whose code is not its analytic class, and with
 // `recheck` every photon marked RISK_RECHECK, is appended to `list` and counted in q->flagged.

@@ -69,7 +69,10 @@ cudaError_t flag_boundary(const Image* images, int n_images, long long total, co
 // `list`), the reference-order kernel whose blocks fill an SM each, and the check of the mixed
 // results against the analytic classes (disagreements appended to `list`).
 cudaError_t risk_prepass(const Image* images, int n_images, long long total, const double* Y0, unsigned char* risk,
-                         long long* list, Queue* q, cudaStream_t s);
+                         long long* list, Queue* q, long long* near_list, Queue* q_near, cudaStream_t s);
+// One block of 384 threads per SM in fast FP64 (its registers fill the SM): the near-edge
+// photons of the mixed pipeline, on SMs of their own beside the mixed trace.
+const Variant* near_wide_variant();
 const Variant* ref_wide_variant();
 cudaError_t check_risk(const Image* images, int n_images, long long total, const unsigned char* risk,
                        const long long* state, long long* list, Queue* q, bool recheck, cudaStream_t s);

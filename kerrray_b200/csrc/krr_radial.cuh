@@ -28,7 +28,9 @@
 
 namespace krr {
 
-enum : int { RISK_ESCAPE = 0, RISK_CAPTURE = 1, RISK_CRITICAL = 2, RISK_RECHECK = 3 };
+// RISK_NEAR: an escaping photon within the near-edge band (near_band) of the boundary; its
+// terminal state, not its class, needs FP64 (the mixed pipeline traces it in fast FP64).
+enum : int { RISK_ESCAPE = 0, RISK_CAPTURE = 1, RISK_CRITICAL = 2, RISK_RECHECK = 3, RISK_NEAR = 4 };
 
 #if defined(__CUDACC__)
 #define KRR_HD __host__ __device__
@@ -80,7 +82,9 @@ KRR_HD inline int radial_minima(const RadialPoly& R, double out[2]) {
 // outside the capture radius, with |L| not negligible against their impact parameter (an
 // axis-crossing ray ends OUT_OF_DOMAIN), are classified; anything else, and any non-finite
 // intermediate, is critical.
-KRR_HD inline int radial_risk(double mass, double a, double r_capture, const double y0[8], double tau_b) {
+// With tau_near > tau_b, an escaping photon within tau_near of the boundary is RISK_NEAR.
+KRR_HD inline int radial_risk(double mass, double a, double r_capture, const double y0[8], double tau_b,
+                              double tau_near = 0.0) {
   const double r0 = y0[1], th = y0[2], pt = y0[4], pr = y0[5], pth = y0[6], pph = y0[7];
   if (!(pr < 0.0) || !(r0 > r_capture)) return RISK_CRITICAL;
   const double e = -pt;
@@ -115,11 +119,18 @@ KRR_HD inline int radial_risk(double mass, double a, double r_capture, const dou
   const double dr_dlam = -2.0 * a * (rm * rm + a2 - a * lam) - 2.0 * dlt * (lam - a);
   const double sens = fabs(dr_dlam) + 2.0 * b * fabs(dr_deta);
   if (!(fabs(vmin) > tau_b * sens)) return RISK_CRITICAL;
+  if (vmin < 0.0 && !(fabs(vmin) > tau_near * sens)) return RISK_NEAR;
   return vmin < 0.0 ? RISK_ESCAPE : RISK_CAPTURE;
 }
 
 // The band of the mixed pipeline (M): a hundred times the integration's error in the impact
 // parameter at rtol 1e-6 and above, scaled with rtol beyond.
 KRR_HD inline double risk_band(double mass, double rtol) { return mass * fmax(2e-3, 2e3 * rtol); }
+
+// The near-edge band of the mixed pipeline (M): escaping photons this close to the boundary
+// pass near the unstable photon orbit, where -dH/dr is a small difference of large terms and
+// the orbit magnifies the FP32 stages' round-off in the exit direction beyond 10 rtol (at
+// rtol 1e-6 on an a* = 0.99, i = 85 deg image, every such photon lay within 0.3 M).
+KRR_HD inline double near_band(double mass) { return 0.3 * mass; }
 
 }  // namespace krr

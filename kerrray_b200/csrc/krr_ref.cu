@@ -45,19 +45,23 @@ __device__ __forceinline__ void append_flagged(bool flag, long long g, long long
 
 __global__ void k_risk_prepass(const Image* __restrict__ images, int n_images, long long total,
                                const double* __restrict__ Y0, unsigned char* __restrict__ risk,
-                               long long* __restrict__ list, Queue* q) {
+                               long long* __restrict__ list, Queue* q, long long* __restrict__ near_list,
+                               Queue* q_near) {
   const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  bool critical = false;
+  bool critical = false, near = false;
   if (g < total) {
     const int img = find_image(images, n_images, g);
     const Params& P = images[img].P;
     double y0[8];
     photon_source(images, img, Y0, g, y0, q);
-    const int cls = radial_risk(P.mass, P.a, P.r_capture, y0, risk_band(P.mass, P.rtol));
+    const int cls = radial_risk(P.mass, P.a, P.r_capture, y0, risk_band(P.mass, P.rtol),
+                                near_list ? near_band(P.mass) : 0.0);
     risk[g] = (unsigned char)cls;
     critical = cls == RISK_CRITICAL;
+    near = cls == RISK_NEAR;
   }
   append_flagged(critical, g, list, q);
+  if (near_list) append_flagged(near, g, near_list, q_near);
 }
 
 __global__ void k_check_risk(const Image* __restrict__ images, int n_images, long long total,
@@ -68,7 +72,7 @@ __global__ void k_check_risk(const Image* __restrict__ images, int n_images, lon
   if (g < total) {
     const int cls = risk[g];
     const long long st = state[g];
-    if (cls == RISK_ESCAPE) flag = st != ESCAPED;
+    if (cls == RISK_ESCAPE || cls == RISK_NEAR) flag = st != ESCAPED;
     else if (cls == RISK_CAPTURE) flag = st != CAPTURED;
     else if (cls == RISK_RECHECK) flag = recheck != 0;
   }
@@ -76,10 +80,11 @@ __global__ void k_check_risk(const Image* __restrict__ images, int n_images, lon
 }
 
 cudaError_t risk_prepass(const Image* images, int n_images, long long total, const double* Y0, unsigned char* risk,
-                         long long* list, Queue* q, cudaStream_t s) {
+                         long long* list, Queue* q, long long* near_list, Queue* q_near, cudaStream_t s) {
   if (total <= 0) return cudaSuccess;
   const int block = 256;  // a multiple of 32: the append is warp-aggregated
-  k_risk_prepass<<<(unsigned)((total + block - 1) / block), block, 0, s>>>(images, n_images, total, Y0, risk, list, q);
+  k_risk_prepass<<<(unsigned)((total + block - 1) / block), block, 0, s>>>(images, n_images, total, Y0, risk, list, q,
+                                                                          near_list, q_near);
   return cudaGetLastError();
 }
 

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol() -> None:
     lib = _lib.lib()
     for name in declared:
         assert hasattr(lib, name), name
-    assert lib.krr_abi_version() == 4
+    assert lib.krr_abi_version() == 5
 
 
 def test_library_is_built_for_sm_100a() -> None:
