@@ -646,23 +646,26 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     if (precision == KRR_PREC_MIXED) {
       // Escaping photons near the shadow edge (krr_radial.cuh:near_band) pass near the
       // unstable photon orbit, which magnifies the FP32 stages' round-off in their exit
-      // direction: they are traced in fast FP64 by a third kernel, launched after the critical
-      // one in the same way (one block fills an SM, programmatic dependent launch, the next
-      // kernel launching as soon as its blocks run), and the mixed trace skips them.  It
-      // waits for the critical kernel at its exit, so the mixed trace's exit wait covers both.
+      // direction: they are traced in fast FP64 by a third kernel, and the mixed trace skips
+      // them.  It is launched first, one block filling each of a fifth of the SMs, and lets the
+      // critical kernel launch as soon as its blocks run; the critical kernel, launched as its
+      // programmatic dependent, waits for it at its own exit, so the mixed trace's exit wait
+      // covers all three.  Its blocks exit when its short queue is drained, and the mixed
+      // trace's waiting blocks take their SMs.
       const krr::Variant* nv = krr::near_wide_variant();
       if (nv->occupancy() < 1) return fail(KRR_ERR_UNSUPPORTED, "the near-edge kernel cannot be resident");
       p.near = true;
       p.near_v = nv;
       p.nearby = p.crit;
       p.nearby.q = p.w.q4;
-      p.nearby.grid = std::max(1, std::min(sms - crit_sms - 1, (sms * 12 + 50) / 100));
+      p.nearby.grid = std::max(1, std::min(sms - crit_sms - 1, sms / 5));
       p.nearby.block = nv->block;
       p.nearby.index = p.w.near_list;
       p.nearby.d_total = &p.w.q4->flagged;
       p.nearby.risk = p.w.risk;  // a photon ending near a budget is marked for the re-check
       p.nearby.flags = krr::TRACE_SPREAD;
-      p.nearby.pdl = krr::PDL_TRIGGER | krr::PDL_WAIT;
+      p.nearby.pdl = krr::PDL_TRIGGER;
+      p.crit.pdl |= krr::PDL_WAIT;
       p.main.flags |= krr::TRACE_SKIP_NEAR;
     }
   }
@@ -680,8 +683,8 @@ cudaError_t enqueue_critical(const Pipeline& p, cudaStream_t s, cudaEvent_t ev0,
   if (e == cudaSuccess)
     e = krr::risk_prepass(p.w.images, p.n_images, p.total, p.main.Y0, p.w.risk, p.w.list, p.w.q1,
                           p.near ? p.w.near_list : nullptr, p.w.q4, s);
-  if (e == cudaSuccess) e = p.crit_v->run(p.crit, s);  // critical photons, reference order
   if (e == cudaSuccess && p.near) e = p.near_v->run(p.nearby, s);  // near-edge photons, fast FP64
+  if (e == cudaSuccess) e = p.crit_v->run(p.crit, s);  // critical photons, reference order
   if (e == cudaSuccess) e = p.main_v->run(p.main, s);  // programmatic dependent: runs beside it
   if (e == cudaSuccess && ev1) e = cudaEventRecord(ev1, s);
   if (e == cudaSuccess) e = krr::check_risk(p.w.images, p.n_images, p.total, p.w.risk, state, p.w.list, p.w.q2, false, s);
