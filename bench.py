@@ -457,14 +457,15 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024", orac
                                                    retrace=retrace))
 
     crit, edge, bare = mixed_with(K.RETRACE_CRITICAL), mixed_with(K.RETRACE_EDGE), mixed_with(0)
+    near = mixed_with(K.RETRACE_CRITICAL_NEAR)
     fast = K.DeviceSweep(specs, precision="fast64", device=local, launch=K.autotune(specs, precision="fast64", device=local)[0])
-    sweeps = (crit, edge, bare, fast)
+    sweeps = (crit, edge, bare, fast, near)
     for sw in sweeps:
         sw.run()
-    t = {k: min(_timed_steps(sw, 3, stream, flush)) for k, sw in zip(("crit", "edge", "bare", "fast"), sweeps)}
+    t = {k: min(_timed_steps(sw, 3, stream, flush)) for k, sw in zip(("crit", "edge", "bare", "fast", "near"), sweeps)}
     plain, t["plain"], plain_block, plain_by_block = best_plain(K, specs, local, stream, flush, 2)
     fplain, t["fast_plain"], fplain_block, _ = best_plain(K, specs, local, stream, flush, 2, precision="fast64")
-    cs, es, bs = crit.stats(), edge.stats(), bare.stats()
+    cs, es, bs, ns = crit.stats(), edge.stats(), bare.stats(), near.stats()
     from kerrray_b200 import _lib
 
     mixed_tflops = algorithmic_flops(bs) / (t["bare"] * 1e-3) / 1e12
@@ -492,9 +493,15 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024", orac
            "speedup_fast64_persistent_vs_fast64_plain": t["fast_plain"] / t["fast"],
            "mask_identical": bool(torch.equal(crit.tensors["state"], ref)),
            "pixels_differing": int((crit.tensors["state"] != ref).sum().item()),
-           "critical": int(cs["critical"]), "rechecked": int(cs["rechecked"]),
+           "critical": int(cs["critical"]), "rechecked": int(cs["rechecked"]), "critical_ms": cs["critical_ms"],
            "pipeline": "analytic critical set in reference-order FP64 beside the mixed trace, then a re-trace of "
                        "every photon unlike its analytic class",
+           "mixed_near_pipeline_rays_s": total / (t["near"] * 1e-3),
+           "speedup_mixed_near_vs_plain": t["plain"] / t["near"],
+           "mixed_near_mask_identical": bool(torch.equal(near.tensors["state"], ref)),
+           "near_edge": int(ns["near_edge"]), "near_critical_ms": ns["critical_ms"],
+           "near_pipeline": "the same with the escaping photons within 0.3 M of the critical curve in fast FP64 "
+                            "on SMs of their own (exit directions at the oracle's bar)",
            "mixed_kernel_only_rays_s": total / (t["bare"] * 1e-3),
            "mixed_kernel_roofline": {"achieved": mixed_tflops, "unit": "TFLOP/s", "fp32_peak": peak32,
                                      "frac_fp32": mixed_tflops / peak32, "fp64_peak": peak64,
@@ -524,6 +531,11 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024", orac
                                              "mixed_pipeline": int((st_mixed != ora_state).sum()),
                                              "fast64": int((st_fast != ora_state).sum())}
         out["mixed_vs_oracle"] = against_oracle(K, spec, pixels, st_mixed, dirs_m, ora)
+        st_near = near.tensors["state"].cpu().numpy()
+        out["pixels_differing_vs_oracle"]["mixed_near_pipeline"] = int((st_near != ora_state).sum())
+        out["mixed_near_vs_oracle"] = against_oracle(K, spec, pixels, st_near,
+                                                     surface_directions(K, spec, near.tensors["Y"], near.tensors["state"]),
+                                                     ora)
         dirs_f = surface_directions(K, spec, fast.tensors["Y"], fast.tensors["state"])
         out["fast64_vs_oracle"] = against_oracle(K, spec, pixels, st_fast, dirs_f, ora)
         out["plain_vs_oracle"] = against_oracle(K, spec, pixels, st_plain, dirs_p, ora)
@@ -660,6 +672,9 @@ def run_ours(args) -> None:
             extra[f"mixed_vs_plain_{name[-4:]}"] = m
             summary[f"mixed_{name[-4:]}"] = {
                 "speedup_vs_plain_fp64": m["speedup_mixed_vs_plain"],
+                "near_band_speedup_vs_plain_fp64": m["speedup_mixed_near_vs_plain"],
+                "near_band_escaped_beyond_10rtol_vs_oracle": m.get("mixed_near_vs_oracle", {}).get("beyond_10rtol"),
+                "near_band_escaped_beyond_bar_vs_oracle": m.get("mixed_near_vs_oracle", {}).get("beyond_bar"),
                 "speedup_vs_fast64_plain": m["speedup_mixed_vs_fast64_plain"],
                 "speedup_vs_fast64_persistent": m["speedup_mixed_vs_fast64_persistent"],
                 "mask_identical_vs_plain": m["mask_identical"], "pixels_differing_vs_plain": m["pixels_differing"],

@@ -62,14 +62,16 @@ enum {
   KRR_RETRACE_NONE = 0,
   KRR_RETRACE_EDGE = 1,     /* after the trace: every pixel that did not end ESCAPED or CAPTURED or
                                whose code differs from one of its 8 neighbours */
-  KRR_RETRACE_CRITICAL = 2  /* before the trace, each photon's analytic class from its constants of
+  KRR_RETRACE_CRITICAL = 2, /* before the trace, each photon's analytic class from its constants of
                                motion (radial potential R(r)); photons within a band of the
                                critical curve run in reference order on SMs of their own, beside
-                               the main trace (and, for a mixed trace, escaping photons within
-                               0.3 M of it in fast FP64 on SMs of their own too); afterwards photons
-                               whose code is not their analytic class are traced again in FP64, and
-                               what still disagrees (or ended within 1 % of its affine or step
-                               budget) in reference order */
+                               the main trace; afterwards photons whose code is not their analytic
+                               class are traced again in FP64, and what still disagrees (or ended
+                               within 1 % of its affine or step budget) in reference order: the
+                               plain FP64 kernel's mask */
+  KRR_RETRACE_CRITICAL_NEAR = 3  /* KRR_RETRACE_CRITICAL and, for a mixed trace, the escaping photons
+                               within 0.3 M of the critical curve traced in fast FP64 on SMs of their
+                               own as well: exit directions within the oracle's bar there too */
 };
 
 /* termination codes (photons/classification.py:60-69) */
@@ -172,9 +174,9 @@ typedef struct krr_stats {
   uint64_t speculative; /* krr_bisect_edges: photons traced ahead of their bracket by idle lanes */
   uint64_t discarded_attempts; /* krr_bisect_edges: attempts of those photons whose side was not
                                   taken (not in `attempts`, which counts the sequential bisection's) */
-  uint64_t near_edge;   /* KRR_RETRACE_CRITICAL with KRR_PREC_MIXED: escaping photons within the
-                           near-edge band of the shadow boundary, traced in fast FP64 beside the
-                           mixed trace (their exit directions need FP64) */
+  uint64_t near_edge;   /* KRR_RETRACE_CRITICAL_NEAR with KRR_PREC_MIXED: escaping photons within
+                           the near-edge band of the shadow boundary, traced in fast FP64 beside
+                           the mixed trace (their exit directions need FP64) */
   uint64_t near_edge_attempts;
 } krr_stats;
 

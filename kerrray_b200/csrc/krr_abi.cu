@@ -549,8 +549,12 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
   p.plain = launch && launch->plain;
   p.plain_block = (launch && launch->block > 0 && launch->block % 32 == 0) ? launch->block : 128;
   p.retrace_mode = launch ? launch->retrace : 0;
-  if (p.retrace_mode < KRR_RETRACE_NONE || p.retrace_mode > KRR_RETRACE_CRITICAL)
-    return fail(KRR_ERR_INVALID, "retrace must be 0, 1 (edge) or 2 (critical), got %d", p.retrace_mode);
+  if (p.retrace_mode < KRR_RETRACE_NONE || p.retrace_mode > KRR_RETRACE_CRITICAL_NEAR)
+    return fail(KRR_ERR_INVALID, "retrace must be 0, 1 (edge), 2 (critical) or 3 (critical and near-edge), got %d",
+                p.retrace_mode);
+  // KRR_RETRACE_CRITICAL_NEAR is the critical-set pipeline with the near-edge band.
+  const bool near_band = p.retrace_mode == KRR_RETRACE_CRITICAL_NEAR;
+  if (near_band) p.retrace_mode = KRR_RETRACE_CRITICAL;
   p.retrace = p.retrace_mode != KRR_RETRACE_NONE;
   if (p.retrace && (p.rk4 || p.dtype32 || p.plain))
     return fail(KRR_ERR_UNSUPPORTED, "the FP64 re-trace follows persistent rk45 float64 launches only");
@@ -643,7 +647,7 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
     p.re.grid = sms * p.re_v->occupancy();
     p.re.block = p.re_v->block;
     p.re.d_total = &p.w.q3->flagged;
-    if (precision == KRR_PREC_MIXED) {
+    if (near_band && precision == KRR_PREC_MIXED) {
       // Escaping photons near the shadow edge (krr_radial.cuh:near_band) pass near the
       // unstable photon orbit, which magnifies the FP32 stages' round-off in their exit
       // direction: they are traced in fast FP64 by a third kernel, and the mixed trace skips

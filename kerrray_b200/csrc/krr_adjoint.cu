@@ -365,7 +365,16 @@ __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(
     }
   }
   // 4. reverse sweep, segment by segment from the last
-  double seg[64][NV];  // states of one segment (K <= 64)
+  // The segment's states (K <= 64): r, theta, p_r, p_theta only -- t and phi do not enter the
+  // right-hand side, so the recomputed steps and the stage inputs need neither.
+  constexpr int NS = 4;
+  double seg[64][NS];
+  auto seg_put = [&](int j, const double y[NV]) {
+    seg[j][0] = y[CR];
+    seg[j][1] = y[CTH];
+    seg[j][2] = y[CPR];
+    seg[j][3] = y[CPTH];
+  };
   for (int c0 = (N - 1) / A.K; c0 >= 0; --c0) {
     const int n0 = c0 * A.K, n1 = min(N, n0 + A.K);
     Ray<Fast64> rs_ray = ry;
@@ -374,15 +383,18 @@ __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(
     Fast64::init_rhs(P, rs_ray.y, rs_ray.pt, rs_ray.pph, rs_ray.sh, rs_ray.f, rs_ray.tr);
     double acc[6][NV], k[6][NV];
     for (int n = n0; n < n1; ++n) {
-#pragma unroll
-      for (int i = 0; i < NV; ++i) seg[n - n0][i] = rs_ray.y[i];
+      seg_put(n - n0, rs_ray.y);
       if (n + 1 < n1) fixed_step(P, rs_ray, tape_h[n], acc, k);
     }
     for (int n = n1 - 1; n >= n0; --n) {
       const double h = tape_h[n];
       Ray<Fast64> st = ry;
-#pragma unroll
-      for (int i = 0; i < NV; ++i) st.y[i] = seg[n - n0][i];
+      st.y[CT] = 0.0;
+      st.y[CPH] = 0.0;
+      st.y[CR] = seg[n - n0][0];
+      st.y[CTH] = seg[n - n0][1];
+      st.y[CPR] = seg[n - n0][2];
+      st.y[CPTH] = seg[n - n0][3];
       Fast64::init_rhs(P, st.y, st.pt, st.pph, st.sh, st.f, st.tr);
       fixed_step(P, st, h, acc, k);
       // Reverse of: Y_s = y + h acc_s (s = 1..5 -> k_s = f(Y_s)); y_new = y + h acc_6; the
@@ -405,10 +417,10 @@ __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(
         }
         const int sm = s - 1;  // acc index of stage input s
         // The stage input exactly as the forward formed it (upd<Fast64>: one fused step).
-        const double Yr = fma(h, acc[sm][CR], seg[n - n0][CR]);
-        const double Yth = fma(h, acc[sm][CTH], seg[n - n0][CTH]);
-        const double Ypr = fma(h, acc[sm][CPR], seg[n - n0][CPR]);
-        const double Ypth = fma(h, acc[sm][CPTH], seg[n - n0][CPTH]);
+        const double Yr = fma(h, acc[sm][CR], seg[n - n0][0]);
+        const double Yth = fma(h, acc[sm][CTH], seg[n - n0][1]);
+        const double Ypr = fma(h, acc[sm][CPR], seg[n - n0][2]);
+        const double Ypth = fma(h, acc[sm][CPTH], seg[n - n0][3]);
         rhs_vjp(m, a, Yr, Yth, ry.pt, Ypr, Ypth, ry.pph, v, ybar_s, abar);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
@@ -429,8 +441,7 @@ __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(
         for (int c = 0; c < NC; ++c)
 #pragma unroll
           for (int i = 0; i < NV; ++i) v[c][i] = kbar[c][0][i];
-        rhs_vjp(m, a, seg[n - n0][CR], seg[n - n0][CTH], ry.pt, seg[n - n0][CPR], seg[n - n0][CPTH], ry.pph, v, xbar,
-                abar);
+        rhs_vjp(m, a, seg[n - n0][0], seg[n - n0][1], ry.pt, seg[n - n0][2], seg[n - n0][3], ry.pph, v, xbar, abar);
       }
     }
   }

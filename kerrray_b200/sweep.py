@@ -27,10 +27,11 @@ from kerrray_b200.camera import Camera
 from kerrray_b200.types import BatchResult, TerminationState
 
 __all__ = ["ImageSpec", "SweepResult", "DeviceSweep", "LaunchConfig", "order_by_cost", "trace_images", "RETRACE_EDGE",
-           "RETRACE_CRITICAL", "analytic_classes", "escape_directions", "trig_eval"]
+           "RETRACE_CRITICAL", "RETRACE_CRITICAL_NEAR", "analytic_classes", "escape_directions", "trig_eval"]
 
 RETRACE_EDGE = 1
 RETRACE_CRITICAL = 2
+RETRACE_CRITICAL_NEAR = 3
 
 
 def escape_directions(spacetime, Y, state, r_surface: float):
@@ -135,7 +136,9 @@ class LaunchConfig:
     # Settle the pixels a mixed trace could classify differently with the reference-order FP64
     # kernel: 0 off; 1 (RETRACE_EDGE) afterwards, every pixel not ESCAPED or CAPTURED or unlike a
     # neighbour; 2 (RETRACE_CRITICAL) the photons near the critical curve (analytic classes from
-    # the radial potential) beside the main trace, then every photon unlike its class.
+    # the radial potential) beside the main trace, then every photon unlike its class;
+    # 3 (RETRACE_CRITICAL_NEAR) that and, for a mixed trace, the escaping photons within 0.3 M of
+    # the critical curve in fast FP64 (their exit directions then meet the oracle's bar too).
     retrace: int = 0
     critical_sms: int = 0     # RETRACE_CRITICAL: SMs of the reference-order kernel (0: library default)
 
