@@ -958,7 +958,7 @@ def run_bisect(args) -> None:
 # rays (forward pass with landing; checkpointed reverse sweep and camera chain), from their FP64
 # instruction counts in one ncu capture of this workload (dadd + dmul + 2 dfma thread
 # instructions of both launches, divided by the rays' 17,650,736 accepted steps; profiles/).
-LENS_FLOP_PER_STEP = 5161
+LENS_FLOP_PER_STEP = 5193
 
 
 def _fd_error(jac: np.ndarray, fd: np.ndarray) -> np.ndarray:
