@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define KRR_ABI_VERSION 5
+#define KRR_ABI_VERSION 6
 
 #if defined(__GNUC__)
 #define KRR_API __attribute__((visibility("default")))
@@ -286,10 +286,18 @@ KRR_API int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_c
  * (escape radius, or capture radius) from the last accepted state by one step along the flow --
  * and its Jacobian d(theta_e, phi_e)/d(alpha, beta, spin, theta_o [rad]) (jac: n x 2 x 4), by the
  * adjoint of the discretised Dormand-Prince 5(4) map over the recorded accepted steps with the
- * controller held fixed, checkpoints every `checkpoint_every` steps and recomputation in the
- * reverse sweep.  FP64.  No counterpart in the reference (its gradients are finite
- * differences of raytracing/backends/numba_backend.py runs).  Device buffers; `workspace` holds
- * the tape (krr_lensing_workspace_size bytes) and must be kept for krr_lensing_replay.
+ * controller held fixed.  FP64.  No counterpart in the reference (its gradients are finite
+ * differences of raytracing/backends/numba_backend.py runs).  Device buffers; `workspace` (256-byte
+ * aligned, as cudaMalloc returns it) holds the tape and must be kept for krr_lensing_replay.
+ * The tape: every accepted step's size, the state every `checkpoint_every` steps, and -- in
+ * whatever workspace lies beyond krr_lensing_workspace_size bytes -- a pool of stage records
+ * (the six stage inputs of each step, 240 B per step, in 16-step chunks).  A ray whose records
+ * all fit is swept back from them; the others recompute each checkpoint segment in the reverse
+ * sweep (the same derivative to rounding, several times slower).  krr_lensing_workspace_size
+ * is the minimum (no pool); krr_lensing_workspace_size_staged adds a pool for `stage_steps`
+ * accepted steps in all (their sum over the rays, plus one chunk of rounding per ray).  The rays
+ * in flight take chunks first come, first served, so a pool well short of the total keeps
+ * whole record sets only for the rays that finish before it runs out.
  * status[k]: 0 ok, 1 more accepted steps than tape_capacity, 2 neither ESCAPED nor CAPTURED. */
 typedef struct krr_lens_params {
   double mass, spin;
@@ -299,10 +307,17 @@ typedef struct krr_lens_params {
   int32_t tape_capacity;     /* accepted steps recorded per ray */
 } krr_lens_params;
 KRR_API size_t krr_lensing_workspace_size(int64_t n, int32_t tape_capacity, int32_t checkpoint_every);
+KRR_API size_t krr_lensing_workspace_size_staged(int64_t n, int32_t tape_capacity, int32_t checkpoint_every,
+                                                 int64_t stage_steps);
 KRR_API int krr_lensing_adjoint(int device, const krr_lens_params* params, const double* d_alpha, const double* d_beta,
                                 int64_t n, double* d_theta, double* d_phi, double* d_jac, int64_t* d_state,
                                 int64_t* d_n_steps, int32_t* d_status, void* workspace, size_t workspace_bytes,
                                 void* stream);
+/* After krr_lensing_adjoint on this workspace (same params and n): rays swept from the stage
+ * records, pool chunks taken and pool chunks the workspace holds.  Synchronises `stream`. */
+KRR_API int krr_lensing_tape_usage(const krr_lens_params* params, int64_t n, const void* workspace,
+                                   size_t workspace_bytes, int64_t* staged_rays, int64_t* chunks_used,
+                                   int64_t* chunks_total, void* stream);
 /* Re-run the map with the step sequence recorded by the last krr_lensing_adjoint call on this
  * workspace (same n, states and step counts), for other (alpha, beta, spin, inclination): the
  * discrete map the adjoint differentiates, without the controller. */

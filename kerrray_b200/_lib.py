@@ -27,7 +27,8 @@ EXPORTS = (
     "krr_integrate_batch_device", "krr_camera_states", "krr_trace_images", "krr_workspace_size",
     "krr_trace_images_device", "krr_fma_peak", "krr_list_variants", "krr_trace_images_noalloc",
     "krr_plan_create", "krr_plan_launch", "krr_plan_stats", "krr_plan_destroy", "krr_bisect_edges",
-    "krr_lensing_workspace_size", "krr_lensing_adjoint", "krr_lensing_replay", "krr_analytic_classes",
+    "krr_lensing_workspace_size", "krr_lensing_workspace_size_staged", "krr_lensing_adjoint",
+    "krr_lensing_tape_usage", "krr_lensing_replay", "krr_analytic_classes",
     "krr_escape_directions", "krr_trig_eval", "krr_disk_shading",
 )
 

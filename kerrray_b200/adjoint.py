@@ -6,8 +6,9 @@ and phi on the termination surface (the escape radius), located from the last ac
 one step along the flow. :func:`lensing_map` evaluates it with its Jacobian
 d(theta_e, phi_e)/d(alpha, beta, a*, i) by the hand-written adjoint of the discretised
 Dormand-Prince 5(4) map (``krr_lensing_adjoint``: accepted step sizes recorded, controller held
-fixed, checkpoints every K steps, recomputation in the reverse sweep, event-time correction at
-the surface). :class:`LensingFunction` exposes it to ``torch.autograd``; :func:`magnification`
+fixed, the stage inputs of every step kept in a device pool and swept back from there --
+checkpoints every K steps with recomputation for the rays the pool cannot hold -- and the
+event-time correction at the surface). :class:`LensingFunction` exposes it to ``torch.autograd``; :func:`magnification`
 is the inverse determinant of the (alpha, beta) block; :func:`fit_spin_inclination` is a
 Gauss-Newton fit of (a*, i) to a target map.
 
@@ -26,10 +27,13 @@ import numpy as np
 from kerrray_b200 import _lib
 from kerrray_b200.types import IntegratorOptions, TerminationOptions
 
-__all__ = ["LensingFunction", "LensingResult", "edge_distant_rays", "fit_spin_inclination", "lensing_map",
-           "magnification"]
+__all__ = ["DEFAULT_STAGE_STEPS_PER_RAY", "LensingFunction", "LensingResult", "edge_distant_rays",
+           "fit_spin_inclination", "lensing_map", "magnification", "tape_usage"]
 
 DEG = math.pi / 180.0
+# Accepted steps per ray the default stage pool is sized for (240 B each); the pool is shared,
+# so it is the total that counts.  Escaping rays at rtol 1e-10 from r_o = 1000 M take about 320.
+DEFAULT_STAGE_STEPS_PER_RAY = 512
 
 
 class KrrLensParams(ctypes.Structure):
@@ -44,6 +48,11 @@ def _bind():
         vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
         L.krr_lensing_workspace_size.restype = ctypes.c_size_t
         L.krr_lensing_workspace_size.argtypes = [i64, i32, i32]
+        L.krr_lensing_workspace_size_staged.restype = ctypes.c_size_t
+        L.krr_lensing_workspace_size_staged.argtypes = [i64, i32, i32, i64]
+        L.krr_lensing_tape_usage.restype = ctypes.c_int
+        L.krr_lensing_tape_usage.argtypes = [ctypes.POINTER(KrrLensParams), i64, vp, ctypes.c_size_t,
+                                             ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
         L.krr_lensing_adjoint.restype = ctypes.c_int
         L.krr_lensing_adjoint.argtypes = [ctypes.c_int, ctypes.POINTER(KrrLensParams), vp, vp, i64, vp, vp, vp, vp, vp,
                                           vp, vp, ctypes.c_size_t, vp]
@@ -76,8 +85,12 @@ def _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tap
 
 def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float = 1000.0, mass: float = 1.0,
                 integ=None, term=None, checkpoint_every: int = 32, tape_capacity: int = 8192,
-                device: int = 0) -> LensingResult:
-    """Map and Jacobian for image points ``alpha``, ``beta`` (torch float64 tensors on the device)."""
+                stage_steps: int | None = None, device: int = 0) -> LensingResult:
+    """Map and Jacobian for image points ``alpha``, ``beta`` (torch float64 tensors on the device).
+
+    ``stage_steps`` sizes the stage pool in accepted steps over all rays (default
+    ``DEFAULT_STAGE_STEPS_PER_RAY`` per ray; 0: no pool, every ray's sweep recomputes from
+    checkpoints).  Rays beyond the pool fall back to recomputation: same derivative to rounding."""
     import torch
 
     L = _bind()
@@ -86,7 +99,11 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
     b = beta.to(dev, torch.float64).contiguous()
     n = a.numel()
     p = _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tape_capacity)
-    ws_bytes = int(L.krr_lensing_workspace_size(n, p.tape_capacity, p.checkpoint_every))
+    if stage_steps is None:
+        stage_steps = n * DEFAULT_STAGE_STEPS_PER_RAY
+    if stage_steps < 0:
+        raise ValueError(f"stage_steps must be >= 0, got {stage_steps}")
+    ws_bytes = int(L.krr_lensing_workspace_size_staged(n, p.tape_capacity, p.checkpoint_every, int(stage_steps)))
     ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=dev)
     theta = torch.empty(n, dtype=torch.float64, device=dev)
     phi = torch.empty_like(theta)
@@ -100,6 +117,19 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
                                      status.data_ptr(), ws.data_ptr(), ws.numel(), stream))
     jac[:, :, 3] *= DEG  # per degree of inclination
     return LensingResult(theta, phi, jac, state, steps, status, ws, p)
+
+
+def tape_usage(res: LensingResult, device: int = 0) -> dict[str, int]:
+    """Of ``res``'s rays: how many were swept from the stage pool, and the pool's chunks used/held."""
+    import torch
+
+    L = _bind()
+    staged, used, total = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    stream = torch.cuda.current_stream(device).cuda_stream
+    _lib.check(L.krr_lensing_tape_usage(ctypes.byref(res.params), res.theta.numel(), res.workspace.data_ptr(),
+                                        res.workspace.numel(), ctypes.byref(staged), ctypes.byref(used),
+                                        ctypes.byref(total), stream))
+    return {"staged_rays": staged.value, "chunks_used": used.value, "chunks_total": total.value}
 
 
 def replay(res: LensingResult, alpha, beta, spin: float, inclination_deg: float, device: int = 0):

@@ -1218,10 +1218,45 @@ int krr_plan_destroy(krr_plan* plan) {
   return KRR_OK;
 }
 
+// The lensing workspace: step sizes (n, cap), checkpoints (n, cap / K + 1, 6), landed final
+// states (n, 16), the stage tape's chunk table (n, cap / STAGE_CHUNK + 1) int32, staged flags (n),
+// the chunk counter, then the pool: every whole chunk that fits in the bytes that remain.  Every
+// offset is a multiple of 256 B (the bulk copies into the pool need 16 B alignment).
+struct LensLayout {
+  size_t h, ck, rec, tab, staged, counter, pool;
+};
+static LensLayout lens_layout(int64_t n, int32_t cap, int32_t K) {
+  LensLayout l{};
+  size_t o = 0;
+  l.h = o;
+  o += round256((size_t)n * cap * 8);
+  l.ck = o;
+  o += round256((size_t)n * (cap / K + 1) * 6 * 8);
+  l.rec = o;
+  o += round256((size_t)n * 16 * 8);
+  l.tab = o;
+  o += round256((size_t)n * (cap / krr::STAGE_CHUNK + 1) * 4);
+  l.staged = o;
+  o += round256((size_t)n);
+  l.counter = o;
+  o += 256;
+  l.pool = o;
+  return l;
+}
+static constexpr size_t kStageChunkBytes = (size_t)krr::STAGE_CHUNK * krr::STEP_REC * 8;
+
 size_t krr_lensing_workspace_size(int64_t n, int32_t tape_capacity, int32_t checkpoint_every) {
   if (n < 0 || tape_capacity < 1 || checkpoint_every < 1) return 0;
-  const size_t ck = (size_t)(tape_capacity / checkpoint_every + 1) * 6;
-  return round256((size_t)n * tape_capacity * 8) + round256((size_t)n * ck * 8) + round256((size_t)n * 16 * 8);
+  return lens_layout(n, tape_capacity, checkpoint_every).pool;
+}
+
+size_t krr_lensing_workspace_size_staged(int64_t n, int32_t tape_capacity, int32_t checkpoint_every,
+                                         int64_t stage_steps) {
+  if (n < 0 || tape_capacity < 1 || checkpoint_every < 1 || stage_steps < 0) return 0;
+  const size_t base = lens_layout(n, tape_capacity, checkpoint_every).pool;
+  if (stage_steps == 0 || n == 0) return base;
+  const size_t chunks = (size_t)((stage_steps + krr::STAGE_CHUNK - 1) / krr::STAGE_CHUNK) + (size_t)n;
+  return base + chunks * kStageChunkBytes;
 }
 
 static int lens_launch(const krr_lens_params* p, int64_t n, krr::LensLaunch& L, size_t workspace_bytes) {
@@ -1262,6 +1297,8 @@ int krr_lensing_adjoint(int device, const krr_lens_params* params, const double*
   if (n == 0) return KRR_OK;
   if (!d_alpha || !d_beta || !d_theta || !d_phi || !d_jac || !d_state || !d_n_steps || !d_status || !workspace)
     return fail(KRR_ERR_INVALID, "device buffers must not be NULL");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail(KRR_ERR_INVALID, "the workspace must be 256-byte aligned (as cudaMalloc returns it)");
   KRR_CUDA(cudaSetDevice(device));
   L.alpha = d_alpha;
   L.beta = d_beta;
@@ -1271,12 +1308,43 @@ int krr_lensing_adjoint(int device, const krr_lens_params* params, const double*
   L.state = reinterpret_cast<long long*>(d_state);
   L.n_steps = reinterpret_cast<long long*>(d_n_steps);
   L.status = d_status;
-  L.tape_h = static_cast<double*>(workspace);
-  L.tape_ck = reinterpret_cast<double*>(static_cast<char*>(workspace) + round256((size_t)n * L.cap * 8));
-  const size_t ck = (size_t)(L.cap / L.K + 1) * 6;
-  L.final_rec = reinterpret_cast<double*>(static_cast<char*>(workspace) + round256((size_t)n * L.cap * 8) +
-                                          round256((size_t)n * ck * 8));
+  char* w = static_cast<char*>(workspace);
+  const LensLayout lay = lens_layout(n, L.cap, L.K);
+  L.tape_h = reinterpret_cast<double*>(w + lay.h);
+  L.tape_ck = reinterpret_cast<double*>(w + lay.ck);
+  L.final_rec = reinterpret_cast<double*>(w + lay.rec);
+  L.chunk_tab = reinterpret_cast<int*>(w + lay.tab);
+  L.staged = reinterpret_cast<unsigned char*>(w + lay.staged);
+  L.pool_next = reinterpret_cast<unsigned long long*>(w + lay.counter);
+  L.pool = reinterpret_cast<double*>(w + lay.pool);
+  L.pool_chunks = (long long)((workspace_bytes - lay.pool) / kStageChunkBytes);
   KRR_CUDA(krr::lensing_adjoint(L, false, static_cast<cudaStream_t>(stream)));
+  return KRR_OK;
+}
+
+int krr_lensing_tape_usage(const krr_lens_params* params, int64_t n, const void* workspace, size_t workspace_bytes,
+                           int64_t* staged_rays, int64_t* chunks_used, int64_t* chunks_total, void* stream) {
+  krr::LensLaunch L{};
+  int rc = lens_launch(params, n, L, workspace_bytes);
+  if (rc) return rc;
+  if (!staged_rays || !chunks_used || !chunks_total) return fail(KRR_ERR_INVALID, "outputs must not be NULL");
+  const LensLayout lay = lens_layout(n, L.cap, L.K);
+  *chunks_total = (int64_t)((workspace_bytes - lay.pool) / kStageChunkBytes);
+  *staged_rays = 0;
+  *chunks_used = 0;
+  if (n == 0) return KRR_OK;
+  if (!workspace) return fail(KRR_ERR_INVALID, "workspace must not be NULL");
+  const char* w = static_cast<const char*>(workspace);
+  std::vector<unsigned char> flags((size_t)n);
+  unsigned long long used = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  KRR_CUDA(cudaMemcpyAsync(flags.data(), w + lay.staged, (size_t)n, cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaMemcpyAsync(&used, w + lay.counter, sizeof(used), cudaMemcpyDeviceToHost, s));
+  KRR_CUDA(cudaStreamSynchronize(s));
+  int64_t k = 0;
+  for (unsigned char f : flags) k += f ? 1 : 0;
+  *staged_rays = k;
+  *chunks_used = (int64_t)std::min<unsigned long long>(used, (unsigned long long)*chunks_total);
   return KRR_OK;
 }
 

@@ -155,8 +155,9 @@ struct RefMode {
   }
   __device__ static void accepted(const Params&, const S[NV], Shadow&, const Trig&) {}
 
-  // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state).
-  template <bool LAST, class R>
+  // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state);
+  // IDX is the stage's number (1..6).
+  template <bool LAST, int IDX, class R>
   __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
     S ys[NV];
 #pragma unroll
@@ -409,18 +410,24 @@ struct Fast64 {
 
   __device__ static Trig accept_trig(double, const Trig& tr) { return tr; }
 
-  struct Shadow {};
+  // kTape: the shadow records each inner stage input (Fast64 derivatives with a shadow that
+  // has record(): the adjoint's forward pass).
+  struct Shadow {
+    static constexpr bool kTape = false;
+  };
 
   __device__ static void init_rhs(const Params& P, const S y[NV], S pt, S pph, Shadow&, K f[NV], Trig& tr) {
     rhs(P, y[CR], y[CTH], pt, y[CPR], y[CPTH], pph, f, tr);
   }
   __device__ static void accepted(const Params&, const S[NV], Shadow&, const Trig&) {}
 
-  // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state).
-  // Stages 1..5 take sin and cos of their theta from the accepted state's (ry.tr, exact) by a
-  // small-angle shift; the last stage evaluates them exactly at the candidate, whose trig then
-  // serves the classification, the diagnostics and the next step.
-  template <bool LAST, class R>
+  // Right-hand side at the stage input y + h*acc (on LAST also returned in yn: the new state);
+  // IDX is the stage's number (1..6).  Stages 1..5 take sin and cos of their theta from the
+  // accepted state's (ry.tr, exact) by a small-angle shift; the last stage evaluates them
+  // exactly at the candidate, whose trig then serves the classification, the diagnostics and
+  // the next step.  With a recording shadow, stages 1..5 hand (r, p_r, p_theta, sin, cos) of
+  // their input to it.
+  template <bool LAST, int IDX, class R>
   __device__ static void stage(const Params& P, const R& ry, K h, const K acc[NV], K f[NV], Trig& tr, S yn[NV]) {
     S ys[NV];
 #pragma unroll
@@ -435,6 +442,7 @@ struct Fast64 {
     }
     tr.s = s;
     tr.c = c;
+    if constexpr (decltype(ry.sh)::kTape && !LAST) ry.sh.record(IDX, ys[CR], ys[CPR], ys[CPTH], s, c);
     rhs_sc(P, ys[CR], s, c, ry.pt, ys[CPR], ys[CPTH], ry.pph, f);
   }
 
@@ -786,22 +794,22 @@ __device__ __forceinline__ void dp_stages_scalar(const Params& P, const Ray<M>& 
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = c(dp::A10) * k0[i];
     if (acc_rec) store(0);
-    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
+    M::template stage<false, 1>(P, ry, h, acc, k1, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = madd<M>(c(dp::A20) * k0[i], c(dp::A21), k1[i]);
     if (acc_rec) store(1);
-    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
+    M::template stage<false, 2>(P, ry, h, acc, k2, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = madd<M>(madd<M>(c(dp::A30) * k0[i], c(dp::A31), k1[i]), c(dp::A32), k2[i]);
     if (acc_rec) store(2);
-    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
+    M::template stage<false, 3>(P, ry, h, acc, k3, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
       const K a = madd<M>(c(dp::A40) * k0[i], c(dp::A41), k1[i]);
       acc[i] = madd<M>(madd<M>(a, c(dp::A42), k2[i]), c(dp::A43), k3[i]);
     }
     if (acc_rec) store(3);
-    M::template stage<false>(P, ry, h, acc, k4, tr, yn);
+    M::template stage<false, 4>(P, ry, h, acc, k4, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
       const K a = madd<M>(c(dp::A50) * k0[i], c(dp::A51), k1[i]);
@@ -811,14 +819,14 @@ __device__ __forceinline__ void dp_stages_scalar(const Params& P, const Ray<M>& 
       esum[i] = madd<M>(madd<M>(madd<M>(c(dp::E0) * k0[i], c(dp::E2), k2[i]), c(dp::E3), k3[i]), c(dp::E4), k4[i]);
     }
     if (acc_rec) store(4);
-    M::template stage<false>(P, ry, h, acc, k5, tr, yn);
+    M::template stage<false, 5>(P, ry, h, acc, k5, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
       acc[i] = madd<M>(bsum[i], c(dp::B5), k5[i]);
       esum[i] = madd<M>(esum[i], c(dp::E5), k5[i]);
     }
     if (acc_rec) store(5);
-    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
+    M::template stage<true, 6>(P, ry, h, acc, k6, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) esum[i] = madd<M>(esum[i], c(dp::E6), k6[i]);
   } else {
@@ -826,21 +834,21 @@ __device__ __forceinline__ void dp_stages_scalar(const Params& P, const Ray<M>& 
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k0[i];
     if (acc_rec) store(0);
-    M::template stage<false>(P, ry, h, acc, k1, tr, yn);
+    M::template stage<false, 1>(P, ry, h, acc, k1, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = c(0.5) * k1[i];
     if (acc_rec) store(1);
-    M::template stage<false>(P, ry, h, acc, k2, tr, yn);
+    M::template stage<false, 2>(P, ry, h, acc, k2, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = c(1.0) * k2[i];
     if (acc_rec) store(2);
-    M::template stage<false>(P, ry, h, acc, k3, tr, yn);
+    M::template stage<false, 3>(P, ry, h, acc, k3, tr, yn);
 #pragma unroll
     for (int i = 0; i < NV; ++i)
       acc[i] = madd<M>(madd<M>(madd<M>(c(dp::RK4_B0) * k0[i], c(dp::RK4_B1), k1[i]), c(dp::RK4_B2), k2[i]),
                        c(dp::RK4_B3), k3[i]);
     if (acc_rec) store(5);
-    M::template stage<true>(P, ry, h, acc, k6, tr, yn);
+    M::template stage<true, 6>(P, ry, h, acc, k6, tr, yn);
   }
 }
 

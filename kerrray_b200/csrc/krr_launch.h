@@ -42,6 +42,12 @@ cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s);
 
 // Lensing-map adjoint (krr_adjoint.cu): derivatives of the terminal celestial direction with
 // respect to (alpha, beta, spin, theta_o); replay = the recorded step sequence without them.
+// The lensing adjoint's stage tape: per accepted step, six stage inputs of STAGE_REC doubles
+// (r, p_r, p_theta, sin theta, cos theta); pool chunks of STAGE_CHUNK steps.
+constexpr int STAGE_REC = 5;
+constexpr int STEP_REC = 6 * STAGE_REC;
+constexpr int STAGE_CHUNK = 16;
+
 struct LensLaunch {
   Params P;
   double spin, mass, r_o, th_o, ph_o;
@@ -58,6 +64,11 @@ struct LensLaunch {
   double* tape_h;
   double* tape_ck;
   double* final_rec;  // (n, 16) landed final states, written by the forward kernel
+  double* pool;       // stage-tape chunks (pool_chunks x STAGE_CHUNK x STEP_REC doubles)
+  long long pool_chunks;
+  unsigned long long* pool_next;  // chunks handed out (zeroed before the forward kernel)
+  int* chunk_tab;                 // (n, cap / STAGE_CHUNK + 1)
+  unsigned char* staged;          // (n): the ray's whole stage tape is in the pool
 };
 cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s);
 

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol() -> None:
     lib = _lib.lib()
     for name in declared:
         assert hasattr(lib, name), name
-    assert lib.krr_abi_version() == 5
+    assert lib.krr_abi_version() == 6
 
 
 def test_library_is_built_for_sm_100a() -> None:
@@ -186,3 +186,21 @@ def test_batched_trace_writes_the_reference_npz(tmp_path: Path) -> None:
     assert back.camera == big.camera and back.count(K.TerminationState.CAPTURED) == 1250
     assert sw.shadow_image(0).state.shape == (2, 2)
 
+
+
+def test_lensing_workspace_sizes() -> None:
+    """The lensing workspace: the minimum holds no stage pool; the staged size adds whole
+    chunks (16 steps x 240 B) for the requested steps plus one chunk of rounding per ray."""
+    from kerrray_b200 import adjoint as A
+
+    L = A._bind()
+    n, cap, k = 1000, 4096, 32
+    base = L.krr_lensing_workspace_size(n, cap, k)
+    assert base > n * cap * 8 and base % 256 == 0
+    assert L.krr_lensing_workspace_size_staged(n, cap, k, 0) == base
+    chunk = 16 * 6 * 5 * 8
+    for steps in (1, 16, 17, 320_000):
+        extra = L.krr_lensing_workspace_size_staged(n, cap, k, steps) - base
+        assert extra == (-(-steps // 16) + n) * chunk, steps
+    assert L.krr_lensing_workspace_size_staged(n, cap, k, -1) == 0
+    assert L.krr_lensing_workspace_size_staged(-1, cap, k, 10) == 0

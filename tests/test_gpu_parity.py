@@ -663,9 +663,13 @@ def test_adjoint_matches_finite_differences_of_the_recorded_map() -> None:
     spin, incl = 0.8, 60.0
     res = A.lensing_map(alpha, beta, spin, incl, checkpoint_every=32)
     assert int((res.status != 0).sum()) == 0 and bool((res.state == 1).all())
-    # Checkpointing only changes what is recomputed: K = 1 (every state stored) is bit-identical.
-    res1 = A.lensing_map(alpha, beta, spin, incl, checkpoint_every=1)
-    assert np.array_equal(res1.jac.cpu().numpy(), res.jac.cpu().numpy())
+    assert A.tape_usage(res)["staged_rays"] == alpha.numel()  # the default pool holds every ray
+    # Without the stage pool, checkpointing only changes what is recomputed: K = 1 (every state
+    # stored) and K = 32 are bit-identical.
+    ck32 = A.lensing_map(alpha, beta, spin, incl, checkpoint_every=32, stage_steps=0)
+    ck1 = A.lensing_map(alpha, beta, spin, incl, checkpoint_every=1, stage_steps=0)
+    assert A.tape_usage(ck32)["staged_rays"] == 0
+    assert np.array_equal(ck1.jac.cpu().numpy(), ck32.jac.cpu().numpy())
     h = 1e-6
     fd = np.zeros((alpha.numel(), 2, 4))
     for p in range(4):
@@ -679,6 +683,42 @@ def test_adjoint_matches_finite_differences_of_the_recorded_map() -> None:
     err = _fd_error(res.jac.cpu().numpy(), fd)
     print("adjoint vs FD of the recorded map: max", err.max(), "median", np.median(err))
     assert err.max() <= 1e-5
+
+
+def test_adjoint_stage_tape_matches_the_checkpoint_sweep() -> None:
+    """The sweep from the stage records against the sweep that recomputes every segment from its
+    checkpoint: the same forward pass (map values and step counts bit for bit), derivatives equal
+    to rounding (the records hold the forward's own stage values: its shifted sines and cosines,
+    its Newton reciprocals).  A pool of 90 % of the chunks the rays need sweeps some rays each way
+    (the rays in flight take chunks first come, first served: those that finish before the pool
+    runs out keep their records), each ray exactly as one of the two full runs does."""
+    from kerrray_b200 import adjoint as A
+
+    alpha, beta = _lens_rays()
+    n = alpha.numel()
+    spin, incl = 0.8, 60.0
+    full = A.lensing_map(alpha, beta, spin, incl)
+    ck = A.lensing_map(alpha, beta, spin, incl, stage_steps=0)
+    use = A.tape_usage(full)
+    assert use["staged_rays"] == n and 0 < use["chunks_used"] <= use["chunks_total"]
+    for name in ("theta", "phi", "n_steps", "state"):
+        assert torch_equal(getattr(full, name), getattr(ck, name)), name
+    jf, jc = full.jac.cpu().numpy(), ck.jac.cpu().numpy()
+    err = _fd_error(jf, jc)
+    print("stage-tape sweep vs checkpoint sweep: max", err.max(), "median", np.median(err))
+    assert err.max() <= 1e-9
+    needed = int(((full.n_steps + 15) // 16).sum())  # chunks of 16 steps
+    part = A.lensing_map(alpha, beta, spin, incl, stage_steps=16 * (int(0.9 * needed) - n))
+    k = A.tape_usage(part)["staged_rays"]
+    assert 0 < k < n, k
+    jp = part.jac.cpu().numpy()
+    as_full = np.all(jp == jf, axis=(1, 2))
+    as_ck = np.all(jp == jc, axis=(1, 2))
+    assert np.all(as_full | as_ck) and int(as_full.sum()) >= k and int(as_ck.sum()) >= n - k
+
+
+def torch_equal(x, y) -> bool:
+    return bool((x == y).all())
 
 
 def _land(O, spin: float, y: np.ndarray, rs: float) -> np.ndarray:
