@@ -28,7 +28,7 @@ from kerrray_b200 import _lib
 from kerrray_b200.types import IntegratorOptions, TerminationOptions
 
 __all__ = ["DEFAULT_STAGE_STEPS_PER_RAY", "LensingFunction", "LensingResult", "edge_distant_rays",
-           "fit_spin_inclination", "lensing_map", "magnification", "tape_usage"]
+           "fit_spin_inclination", "lensing_map", "magnification", "tape_usage", "workspace_bytes"]
 
 DEG = math.pi / 180.0
 # Accepted steps per ray the default stage pool is sized for (240 B each); the pool is shared,
@@ -85,12 +85,15 @@ def _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tap
 
 def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float = 1000.0, mass: float = 1.0,
                 integ=None, term=None, checkpoint_every: int = 32, tape_capacity: int = 8192,
-                stage_steps: int | None = None, device: int = 0) -> LensingResult:
+                stage_steps: int | None = None, workspace=None, device: int = 0) -> LensingResult:
     """Map and Jacobian for image points ``alpha``, ``beta`` (torch float64 tensors on the device).
 
     ``stage_steps`` sizes the stage pool in accepted steps over all rays (default
     ``DEFAULT_STAGE_STEPS_PER_RAY`` per ray; 0: no pool, every ray's sweep recomputes from
-    checkpoints).  Rays beyond the pool fall back to recomputation: same derivative to rounding."""
+    checkpoints).  Rays beyond the pool fall back to recomputation: same derivative to rounding.
+    ``workspace``: a uint8 tensor on the device to hold the tape instead of a fresh allocation
+    (any size from ``workspace_bytes(...)`` up: bytes beyond the minimum become stage pool); the
+    result keeps it for ``replay`` until the next call given the same tensor."""
     import torch
 
     L = _bind()
@@ -99,12 +102,14 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
     b = beta.to(dev, torch.float64).contiguous()
     n = a.numel()
     p = _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tape_capacity)
-    if stage_steps is None:
-        stage_steps = n * DEFAULT_STAGE_STEPS_PER_RAY
-    if stage_steps < 0:
-        raise ValueError(f"stage_steps must be >= 0, got {stage_steps}")
-    ws_bytes = int(L.krr_lensing_workspace_size_staged(n, p.tape_capacity, p.checkpoint_every, int(stage_steps)))
-    ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=dev)
+    if workspace is not None:
+        need = int(L.krr_lensing_workspace_size(n, p.tape_capacity, p.checkpoint_every))
+        if workspace.dtype != torch.uint8 or workspace.device != dev or workspace.numel() < need:
+            raise ValueError(f"workspace must be a uint8 tensor on {dev} of at least {need} bytes")
+        ws = workspace
+    else:
+        ws = torch.empty(max(workspace_bytes(n, checkpoint_every=checkpoint_every, tape_capacity=tape_capacity,
+                                             stage_steps=stage_steps), 8), dtype=torch.uint8, device=dev)
     theta = torch.empty(n, dtype=torch.float64, device=dev)
     phi = torch.empty_like(theta)
     jac = torch.empty((n, 2, 4), dtype=torch.float64, device=dev)
@@ -117,6 +122,21 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
                                      status.data_ptr(), ws.data_ptr(), ws.numel(), stream))
     jac[:, :, 3] *= DEG  # per degree of inclination
     return LensingResult(theta, phi, jac, state, steps, status, ws, p)
+
+
+def workspace_bytes(n: int, *, checkpoint_every: int = 32, tape_capacity: int = 8192,
+                    stage_steps: int | None = None) -> int:
+    """Bytes of the tape for ``n`` rays with a stage pool of ``stage_steps`` accepted steps in all
+    (default ``DEFAULT_STAGE_STEPS_PER_RAY`` per ray; 0: the minimum, no pool)."""
+    if stage_steps is None:
+        stage_steps = n * DEFAULT_STAGE_STEPS_PER_RAY
+    if stage_steps < 0:
+        raise ValueError(f"stage_steps must be >= 0, got {stage_steps}")
+    size = int(_bind().krr_lensing_workspace_size_staged(int(n), int(tape_capacity), int(checkpoint_every),
+                                                         int(stage_steps)))
+    if size == 0 and n > 0:
+        raise ValueError("invalid tape_capacity or checkpoint_every")
+    return size
 
 
 def tape_usage(res: LensingResult, device: int = 0) -> dict[str, int]:
@@ -215,11 +235,13 @@ def fit_spin_inclination(alpha, beta, target_theta, target_phi, *, p0=(0.5, 50.0
 
     targets_ok = torch.isfinite(target_theta) & torch.isfinite(target_phi)
     evaluations = 0
+    # One tape for every evaluation: the fit reads each result's map and Jacobian, never its tape.
+    ws = torch.empty(workspace_bytes(alpha.numel()), dtype=torch.uint8, device=torch.device("cuda", device))
 
     def evaluate(q):
         nonlocal evaluations
         evaluations += 1
-        res = lensing_map(alpha, beta, float(q[0]), float(q[1]), r_o=r_o, integ=integ, device=device)
+        res = lensing_map(alpha, beta, float(q[0]), float(q[1]), r_o=r_o, integ=integ, workspace=ws, device=device)
         ok = (res.status == 0) & (res.state == 1) & targets_ok
         d_th = res.theta - target_theta
         d_ph = torch.remainder(res.phi - target_phi + math.pi, 2.0 * math.pi) - math.pi

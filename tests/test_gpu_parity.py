@@ -274,9 +274,13 @@ def _spin99_specs(res: int):
 
 
 def _direction_error(d1: np.ndarray, d2: np.ndarray) -> np.ndarray:
-    """max(|d theta|, |d phi| wrapped) per row (rad)."""
-    dph = np.abs(np.remainder(d1[:, 1] - d2[:, 1] + np.pi, 2 * np.pi) - np.pi)
-    return np.maximum(np.abs(d1[:, 0] - d2[:, 0]), dph)
+    """The angle (rad) between the directions (theta, phi) of each row on the escape sphere,
+    2 asin(|u1 - u2| / 2) of their unit vectors (phi alone is ill-conditioned next to a pole)."""
+    def unit(d):
+        s = np.sin(d[:, 0])
+        return np.stack([s * np.cos(d[:, 1]), s * np.sin(d[:, 1]), np.cos(d[:, 0])], axis=1)
+
+    return 2.0 * np.arcsin(np.minimum(1.0, 0.5 * np.linalg.norm(unit(d1) - unit(d2), axis=1)))
 
 
 def _surface_dirs(st, Y, state, r_esc: float) -> np.ndarray:
@@ -287,8 +291,9 @@ def _surface_dirs(st, Y, state, r_esc: float) -> np.ndarray:
 
 
 def _terminal_states_within_the_bar(specs, sweep, hold: bool = True) -> dict:
-    """Every escaped ray of a batched trace against the oracle on the escape surface: within
-    10 rtol, or within 4x the oracle's own envelope there -- the larger of its distance to the
+    """Every escaped ray of a batched trace against the oracle on the escape surface (the angle
+    between their directions): within 10 rtol, or within 4x the oracle's own envelope there in
+    the same measure -- the larger of its distance to the
     oracle at a 100x tighter tolerance and its spread over tolerances 5 % either side (the
     reference's result for a ray whose step sequence takes very large steps changes with any
     change of that sequence)."""
@@ -715,6 +720,18 @@ def test_adjoint_stage_tape_matches_the_checkpoint_sweep() -> None:
     as_full = np.all(jp == jf, axis=(1, 2))
     as_ck = np.all(jp == jc, axis=(1, 2))
     assert np.all(as_full | as_ck) and int(as_full.sum()) >= k and int(as_ck.sum()) >= n - k
+    # A caller's workspace, used twice: the same results; the minimum size holds no pool.
+    import torch
+
+    ws = torch.empty(A.workspace_bytes(n), dtype=torch.uint8, device="cuda")
+    for _ in range(2):
+        again = A.lensing_map(alpha, beta, spin, incl, workspace=ws)
+        assert np.array_equal(again.jac.cpu().numpy(), jf) and A.tape_usage(again)["staged_rays"] == n
+    small = torch.empty(A.workspace_bytes(n, stage_steps=0), dtype=torch.uint8, device="cuda")
+    bare = A.lensing_map(alpha, beta, spin, incl, workspace=small)
+    assert np.array_equal(bare.jac.cpu().numpy(), jc) and A.tape_usage(bare)["staged_rays"] == 0
+    with pytest.raises(ValueError):
+        A.lensing_map(alpha, beta, spin, incl, workspace=small[:1024])
 
 
 def torch_equal(x, y) -> bool:
