@@ -1041,7 +1041,8 @@ def lensing_cpu_baseline(K, a_np: np.ndarray, b_np: np.ndarray, spin: float, inc
             dirs.append(surface_directions(K, (K.Spacetime(1.0, s_), r_o), o["Y"], o["state"]))
         fd[:, :, p_] = (dirs[0] - dirs[1]) / (2 * h)
     line = {"value": idx.size / dt, "unit": "rays/s", "cores": threads, "kind": "port",
-            "sample": (f"every {stride}th of the {a_np.size} rays ({idx.size} rays, {dt:.1f} s): central differences "
+            "sample": ((f"every {stride}th of the {a_np.size} rays" if stride > 1 else f"all {a_np.size} rays") +
+                       f" ({idx.size} rays, {dt:.1f} s): central differences "
                        f"(h = 1e-6) of the oracle's integration, 8 traces per ray at rtol 1e-10, OpenMP {threads} "
                        f"threads")}
     return line, {"idx": idx, "fd": fd}
