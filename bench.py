@@ -733,14 +733,14 @@ def run_ours(args) -> None:
             ("RUNNING", "ESCAPED", "CAPTURED", "MAX_AFFINE", "FAILURE", "OUT_OF_DOMAIN", "DISK_HIT"), counts)}
     if single and args.workload == "sweep":
         # The other two headline workloads, each with its own roofline and CPU baseline.
-        bis = bisect_line(K, argparse.Namespace(steps=3, warmup=1, no_cpu=args.no_cpu, precision="fast64"))
+        bis = bisect_line(K, argparse.Namespace(steps=3, warmup=3, no_cpu=args.no_cpu, precision="fast64"))
         extra["bisect"] = bis
         summary["bisect"] = {"rays_s": bis["value"], "frac_fp64": bis["roofline"]["frac"],
                              "cpu_rays_s": (bis["cpu_baseline"] or {}).get("value"),
                              "edge_rms_over_rtol_median": {k: v["rms_over_rtol_median"]
                                                            for k, v in bis["edge_error_vs_bardeen"].items()}}
         torch.cuda.empty_cache()
-        lens = lensing_line(K, argparse.Namespace(steps=3, warmup=1, no_cpu=args.no_cpu))
+        lens = lensing_line(K, argparse.Namespace(steps=3, warmup=3, no_cpu=args.no_cpu))
         extra["lensing"] = lens
         summary["lensing"] = {"rays_s": lens["value"], "e2e_rays_s": lens["e2e"]["value"],
                               "frac_fp64": (lens["roofline"] or {}).get("frac"),
@@ -762,7 +762,9 @@ def run_ours(args) -> None:
                        "parallelism": (f"shards{world} (the workload replicated per GPU with the observer turned in "
                                        f"azimuth; images cut into pixel pieces of equal predicted cost; no data-path "
                                        f"collective)"),
-                       "launch": {k: v for k, v in chosen.items() if k != "ms"},
+                       "launch": {**{k: v for k, v in chosen.items() if k != "ms"},
+                                  "finalists_full_size_ms": {f"{t['variant']}:{t['refill_threshold']}": t["ms"]
+                                                             for t in tune_report.get("final") or []}},
                        "l2": "256 MB buffer written between timed steps (> 126 MB L2)",
                        "summary": summary},
             "e2e": e2e, "gpu_launches": args.steps,

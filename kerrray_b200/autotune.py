@@ -6,7 +6,11 @@ lanes of a warp may sit idle before the warp pulls new photons from the queue) b
 each candidate on a reduced copy of the workload: the same images at a half or a quarter of the
 resolution per side (same field of view, so the same mix of escaping, captured and
 near-critical photons), reduced only while at least half a million photons remain -- fewer
-leave the launch's tail in charge and favour other shapes than the full workload would. Each
+leave the launch's tail in charge and favour other shapes than the full workload would. The
+reduced copy ranks the candidates; the fastest few are then timed again on the workload itself
+(candidates within a percent or two at a quarter of the resolution need not keep their order
+at full size: a refill threshold of 8 won the reduced sweep once and ran 2 % slower than 4 on the
+full one). Each
 warp handles 32 photons at a time, one per lane; the refill claims as many queue entries as
 the warp has idle lanes.
 
@@ -101,9 +105,12 @@ def tuning_scale(specs: Sequence[ImageSpec]) -> int:
 
 
 def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: int = 0, scale: int | None = None,
-             thresholds: Sequence[int] = (1, 4, 8, 16), repeats: int = 2, use_cache: bool = True) -> tuple[LaunchConfig, dict]:
+             thresholds: Sequence[int] = (1, 4, 8, 16), repeats: int = 2, finalists: int = 3,
+             use_cache: bool = True) -> tuple[LaunchConfig, dict]:
     """Return the fastest ``LaunchConfig`` for ``specs`` and a report of every candidate's time
-    (``scale``: reduction per side of the tuning workload; None chooses ``tuning_scale``)."""
+    (``scale``: reduction per side of the tuning workload; None chooses ``tuning_scale``;
+    ``finalists``: how many of the fastest on the reduced workload are timed on ``specs``
+    itself to decide)."""
     specs = list(specs)
     if scale is None:
         scale = tuning_scale(specs)
@@ -118,22 +125,33 @@ def autotune(specs: Sequence[ImageSpec], *, precision: str = "fast64", device: i
             return LaunchConfig(**table[key]["config"]), table[key]
     small = _reduced(specs, scale) if scale > 1 else specs
     variants = list_variants(precision, specs[0].integ, specs[0].term, device)
+    def timed(images, cfg) -> float:
+        sweep = DeviceSweep(images, precision=precision, launch=cfg, device=device, minimal=True, graph=False)
+        sweep.run()
+        ms = min(sweep.run()["kernel_ms"] for _ in range(repeats))
+        sweep.close()
+        return ms
+
     trials = []
-    best = None
     for v in variants:
         if v["blocks_per_sm"] < 1:
             continue
         for t in thresholds:
-            cfg = LaunchConfig(variant=v["variant"], refill_threshold=t)
-            sweep = DeviceSweep(small, precision=precision, launch=cfg, device=device, minimal=True, graph=False)
-            sweep.run()
-            ms = min(sweep.run()["kernel_ms"] for _ in range(repeats))
+            ms = timed(small, LaunchConfig(variant=v["variant"], refill_threshold=t))
             trials.append({**v, "refill_threshold": t, "ms": ms})
-            if best is None or ms < best[1]:
-                best = (cfg, ms)
-            del sweep
+    ranked = sorted(trials, key=lambda tr: tr["ms"])
+    final = []
+    if scale > 1 and finalists > 1:
+        for tr in ranked[:finalists]:
+            ms = timed(specs, LaunchConfig(variant=tr["variant"], refill_threshold=tr["refill_threshold"]))
+            final.append({"variant": tr["variant"], "refill_threshold": tr["refill_threshold"], "ms": ms})
+        win = min(final, key=lambda tr: tr["ms"])
+    else:
+        win = ranked[0]
+    best = (LaunchConfig(variant=win["variant"], refill_threshold=win["refill_threshold"]), win["ms"])
     report = {"config": {"variant": best[0].variant, "refill_threshold": best[0].refill_threshold},
-              "ms": best[1], "photons": sum(s.n_rays for s in small), "scale": scale, "trials": trials}
+              "ms": best[1], "photons": sum(s.n_rays for s in small), "scale": scale, "trials": trials,
+              "final": final, "final_photons": sum(s.n_rays for s in specs) if final else None}
     _CACHE[key] = report
     if use_cache and os.environ.get("KRR_AUTOTUNE_CACHE"):
         table = _load_file()

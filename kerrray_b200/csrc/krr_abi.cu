@@ -203,6 +203,8 @@ struct Context {
   cudaStream_t h2d_stream = nullptr;    // host-to-device copies of Y0 ahead of the trace
   cudaEvent_t chunk_ev[4] = {};         // the end of each chunk's trace
   cudaEvent_t h2d_ev[4] = {};           // each chunk's Y0 on the device
+  cudaStream_t trace2 = nullptr;        // every other chunk's trace, so consecutive traces overlap their tails
+  cudaEvent_t fork_ev = nullptr;        // trace2 starts after the setup on the main stream
   int sm_count = 0;
   DevBuf buf[B_COUNT];
 };
@@ -228,6 +230,8 @@ int get_context(int device, Context** out) {
     KRR_CUDA(cudaEventCreate(&c->ev2));
     KRR_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     KRR_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
+    KRR_CUDA(cudaStreamCreateWithFlags(&c->trace2, cudaStreamNonBlocking));
+    KRR_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
     for (auto& ev : c->chunk_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     for (auto& ev : c->h2d_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     KRR_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
@@ -802,20 +806,28 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
   const cudaStream_t s = c->stream;
   // Whatever path returns, no copy may still read or write the caller's buffers afterwards.
   struct Drain {
-    cudaStream_t trace, out, in;
+    cudaStream_t trace, trace2, out, in;
     ~Drain() {
       cudaStreamSynchronize(trace);
+      cudaStreamSynchronize(trace2);
       cudaStreamSynchronize(out);
       cudaStreamSynchronize(in);
     }
-  } drain{s, c->copy_stream, c->h2d_stream};
+  } drain{s, c->trace2, c->copy_stream, c->h2d_stream};
   const int chunks = (int)std::min<long long>(4, std::max<long long>(1, total / kChunkPhotons));
-  // Ranges weighted 3:3:...:1: the last range's copy-out is the one not hidden behind a trace.
-  long long bound[5];
-  const long long wsum = 3LL * (chunks - 1) + 1;
-  for (int k = 0; k <= chunks; ++k) bound[k] = (k == chunks) ? total : total * (3LL * k) / wsum;
-  // A host Y0 goes up range by range on its own stream while the host checks it (every value
-  // finite) in parallel; no trace starts before the check has passed.
+  // Ranges weighted 1:3:...:3:1: the first range's upload and the last range's copy-out are the
+  // ones not hidden behind a trace.
+  long long bound[5], wts[4], wsum = 0, acc = 0;
+  for (int k = 0; k < chunks; ++k) wsum += (wts[k] = (k == 0 || k == chunks - 1) ? 1 : 3);
+  for (int k = 0; k <= chunks; ++k) {
+    bound[k] = (k == chunks) ? total : total * acc / wsum;
+    if (k < chunks) acc += wts[k];
+  }
+  // A host Y0 goes up range by range on its own stream.  The host checks it (every value
+  // finite) while the ranges are traced, and a non-finite value fails the call before any result
+  // is copied out: such a photon ends as a NUMERICAL_FAILURE at its first classification, so the
+  // traces it reaches only run to completion.  (Checked before the launches, the scan of a
+  // large sweep's Y0 held back the first trace by ~10 ms.)
   const double* d_Y0 = nullptr;
   if (host_Y0) {
     KRR_CUDA(c->buf[B_Y0].ensure((size_t)total * 8 * sizeof(double)));
@@ -825,7 +837,6 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
       KRR_CUDA(cudaMemcpyAsync(dst + off, host_Y0 + off, n * sizeof(double), cudaMemcpyHostToDevice, c->h2d_stream));
       KRR_CUDA(cudaEventRecord(c->h2d_ev[k], c->h2d_stream));
     }
-    if (!all_finite_parallel(host_Y0, (size_t)total * 8)) return fail(KRR_ERR_INVALID, "Y0 must be finite");
     d_Y0 = dst;
   }
   Pipeline p;
@@ -842,16 +853,24 @@ int run_images_overlapped(Context* c, const krr_image* images, const std::vector
   }
   if (p.out.event_Y) KRR_CUDA(cudaMemsetAsync(p.out.event_Y, 0, (size_t)total * 8 * sizeof(double), s));
   if (p.out.event_hit) KRR_CUDA(cudaMemsetAsync(p.out.event_hit, 0, (size_t)total, s));
+  // Consecutive ranges on alternate streams: a range's persistent blocks start on SMs that the
+  // previous range's blocks leave in its tail (the ranges share no data; each has its own queue).
   KRR_CUDA(cudaEventRecord(c->ev0, s));
+  KRR_CUDA(cudaEventRecord(c->fork_ev, s));
+  KRR_CUDA(cudaStreamWaitEvent(c->trace2, c->fork_ev, 0));
+  const cudaStream_t ts[2] = {s, c->trace2};
   for (int k = 0; k < chunks; ++k) {
+    const cudaStream_t st = ts[k & 1];
     krr::PersistArgs a = p.main;
     a.q = qs[k];
     a.total = bound[k + 1];
-    if (host_Y0) KRR_CUDA(cudaStreamWaitEvent(s, c->h2d_ev[k], 0));
-    KRR_CUDA(p.main_v->run(a, s));
-    KRR_CUDA(cudaEventRecord(c->chunk_ev[k], s));
+    if (host_Y0) KRR_CUDA(cudaStreamWaitEvent(st, c->h2d_ev[k], 0));
+    KRR_CUDA(p.main_v->run(a, st));
+    KRR_CUDA(cudaEventRecord(c->chunk_ev[k], st));
   }
+  for (int k = 1; k < chunks; k += 2) KRR_CUDA(cudaStreamWaitEvent(s, c->chunk_ev[k], 0));
   KRR_CUDA(cudaEventRecord(c->ev1, s));
+  if (host_Y0 && !all_finite_parallel(host_Y0, (size_t)total * 8)) return fail(KRR_ERR_INVALID, "Y0 must be finite");
   // Every launch is queued before the first copy-out: a copy into pageable host memory returns
   // only when it has finished, and must not hold back the next range's launch.
   for (int k = 0; k < chunks; ++k) {

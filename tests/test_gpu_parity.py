@@ -264,6 +264,14 @@ def test_autotuner_picks_a_measured_candidate() -> None:
     cfg, report = K.autotune(specs, precision="fast64", use_cache=False, thresholds=(1, 8), repeats=1)
     assert report["trials"] and report["ms"] == min(t["ms"] for t in report["trials"])
     assert (cfg.variant, cfg.refill_threshold) in {(t["variant"], t["refill_threshold"]) for t in report["trials"]}
+    # ranked on a reduced copy, decided among the fastest few on the images themselves
+    cfg2, rep2 = K.autotune(specs, precision="fast64", use_cache=False, thresholds=(1, 8), repeats=1, scale=2,
+                            finalists=2)
+    ranked = sorted(rep2["trials"], key=lambda t: t["ms"])[:2]
+    assert [(t["variant"], t["refill_threshold"]) for t in rep2["final"]] == [(t["variant"], t["refill_threshold"])
+                                                                             for t in ranked]
+    win = min(rep2["final"], key=lambda t: t["ms"])
+    assert (cfg2.variant, cfg2.refill_threshold) == (win["variant"], win["refill_threshold"]) and rep2["ms"] == win["ms"]
 
 
 def _spin99_specs(res: int):
@@ -557,14 +565,24 @@ def test_trace_images_with_overlapped_copies_is_one_launch() -> None:
     dev.run()
     for name in ("state", "Y", "n_steps", "n_rejected", "lam", "max_null_error"):
         assert np.array_equal(host.arrays[name], dev.tensors[name].cpu().numpy()), name
-    # a host Y0 goes up range by range, checked on the host before any range is traced
+    # a host Y0 goes up range by range, checked on the host while the ranges are traced
     y0 = K.initial_states(spec.camera, spec.spacetime)
     from_y0 = K.trace_images([spec], precision="fast64", launch=launch, Y0=y0)
     assert np.array_equal(from_y0.arrays["state"], host.arrays["state"])
     assert np.array_equal(from_y0.arrays["Y"], host.arrays["Y"])
+    # a non-finite value fails the call, and no result reaches the caller's buffers
     y0[3_000_000, 6] = np.nan
+    n = y0.shape[0]
+    outs = {"Y": np.full((n, 8), -7.0), "state": np.full(n, -7, dtype=np.int64), "n_steps": np.full(n, -7, dtype=np.int64),
+            "n_rejected": np.full(n, -7, dtype=np.int64), "lam": np.full(n, -7.0), "max_null_error": np.full(n, -7.0),
+            "max_energy_drift": np.full(n, -7.0), "max_lz_drift": np.full(n, -7.0), "max_carter_drift": np.full(n, -7.0),
+            "event_Y": None, "event_hit": None}
     with pytest.raises(ValueError, match="finite"):
-        K.trace_images([spec], precision="fast64", launch=launch, Y0=y0)
+        K.trace_images([spec], precision="fast64", launch=launch, Y0=y0, out=outs)
+    assert all(np.all(a == -7) for a in outs.values() if a is not None)
+    # and the context stays usable
+    again = K.trace_images([spec], precision="fast64", launch=launch, Y0=K.initial_states(spec.camera, spec.spacetime))
+    assert np.array_equal(again.arrays["Y"], host.arrays["Y"])
     dev.close()
 
 
