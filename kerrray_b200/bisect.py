@@ -28,7 +28,7 @@ from kerrray_b200.boundary import finite_distance_scale
 from kerrray_b200.orbits import BardeenCurve
 from kerrray_b200.types import IntegratorOptions, TerminationOptions
 
-__all__ = ["EdgeCase", "bisect_edge", "bisect_edges", "edge_options", "edge_study"]
+__all__ = ["EdgeCase", "bisect_edge", "bisect_edges", "edge_options", "edge_study", "item_cost"]
 
 
 def edge_options(rtol: float, r_o: float) -> tuple[IntegratorOptions, TerminationOptions]:
@@ -58,23 +58,43 @@ class EdgeCase:
                                 centre_beta=float(self.centre[1]))
 
 
+def item_cost(case: EdgeCase) -> float:
+    """Predicted cost of one of the case's directions relative to others: rtol^(-1/5), the
+    controller's step count scaling (the same model shards the items over ranks)."""
+    return float(case.rtol) ** -0.2
+
+
 def bisect_edges(cases: Sequence[EdgeCase], iterations: int, *, precision: str = "reference",
-                 device: int = 0, item_failures: bool = False) -> tuple[list[tuple[np.ndarray, np.ndarray, object]], dict]:
+                 device: int = 0, item_failures: bool = False,
+                 order: str = "cost") -> tuple[list[tuple[np.ndarray, np.ndarray, object]], dict]:
     """Run every case's bisection in one launch; per case ``(r_mid, width, failures)`` and the stats.
 
     ``failures`` counts the photons of the case that ended neither ESCAPED nor CAPTURED (the
     reference's lost photons); with ``item_failures`` it is that count per direction (an array).
+    ``order="cost"`` hands the launch's work queue the cases' directions most expensive first
+    (``item_cost``), so that the cheap ones make the tail; ``"given"`` keeps the order of
+    ``cases``. Each direction's result does not depend on the order.
     """
     cases = list(cases)
+    if order not in ("cost", "given"):
+        raise ValueError(f"order must be 'cost' or 'given', got {order!r}")
     arr = (_lib.KrrEdgeCase * len(cases))(*[c.struct() for c in cases])
     sizes = [np.asarray(c.angles).size for c in cases]
-    item_case = np.concatenate([np.full(n, k, dtype=np.int32) for k, n in enumerate(sizes)])
-    angles = np.concatenate([np.asarray(c.angles, dtype=np.float64).ravel() for c in cases])
+    seq = list(range(len(cases)))
+    if order == "cost":
+        seq.sort(key=lambda k: -item_cost(cases[k]))  # stable: equal costs keep their order
+    start_of = {}
+    pos = 0
+    for k in seq:
+        start_of[k] = pos
+        pos += sizes[k]
+    item_case = np.concatenate([np.full(sizes[k], k, dtype=np.int32) for k in seq])
+    angles = np.concatenate([np.asarray(cases[k].angles, dtype=np.float64).ravel() for k in seq])
     cos_phi, sin_phi = np.ascontiguousarray(np.cos(angles)), np.ascontiguousarray(np.sin(angles))
-    lo = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(c.r_lo, np.float64), (n,))
-                                              for c, n in zip(cases, sizes)]))
-    hi = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(c.r_hi, np.float64), (n,))
-                                              for c, n in zip(cases, sizes)]))
+    lo = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(cases[k].r_lo, np.float64), (sizes[k],))
+                                              for k in seq]))
+    hi = np.ascontiguousarray(np.concatenate([np.broadcast_to(np.asarray(cases[k].r_hi, np.float64), (sizes[k],))
+                                              for k in seq]))
     fails = np.zeros(lo.size, dtype=np.int64)
     stats = _lib.KrrStats()
     if precision not in _lib.PRECISIONS:
@@ -84,11 +104,9 @@ def bisect_edges(cases: Sequence[EdgeCase], iterations: int, *, precision: str =
                                      int(iterations), _lib.PRECISIONS[precision], ctypes.byref(stats))
     _lib.check(rc)
     out = []
-    start = 0
-    for n in sizes:
-        sl = slice(start, start + n)
+    for k, n in enumerate(sizes):
+        sl = slice(start_of[k], start_of[k] + n)
         out.append((0.5 * (lo[sl] + hi[sl]), hi[sl] - lo[sl], fails[sl].copy() if item_failures else int(fails[sl].sum())))
-        start += n
     return out, stats.as_dict()
 
 
