@@ -73,6 +73,7 @@ class LensingResult:
     status: Any       # (n,) 0 ok, 1 tape full, 2 neither escaped nor captured
     workspace: Any    # the tape (kept for replay)
     params: KrrLensParams
+    perm: Any = None  # the order the rays were traced in (input indices), None: the input order
 
 
 def _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tape_capacity) -> KrrLensParams:
@@ -85,7 +86,8 @@ def _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tap
 
 def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float = 1000.0, mass: float = 1.0,
                 integ=None, term=None, checkpoint_every: int = 32, tape_capacity: int = 8192,
-                stage_steps: int | None = None, workspace=None, device: int = 0) -> LensingResult:
+                stage_steps: int | None = None, workspace=None, order: Any = "impact",
+                device: int = 0) -> LensingResult:
     """Map and Jacobian for image points ``alpha``, ``beta`` (torch float64 tensors on the device).
 
     ``stage_steps`` sizes the stage pool in accepted steps over all rays (default
@@ -93,7 +95,15 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
     checkpoints).  Rays beyond the pool fall back to recomputation: same derivative to rounding.
     ``workspace``: a uint8 tensor on the device to hold the tape instead of a fresh allocation
     (any size from ``workspace_bytes(...)`` up: bytes beyond the minimum become stage pool); the
-    result keeps it for ``replay`` until the next call given the same tensor."""
+    result keeps it for ``replay`` until the next call given the same tensor.
+
+    ``order``: the order the rays are traced in, one ray per thread. A warp lasts as long as its
+    longest ray, so rays of like length belong together, the longest first. ``"impact"`` (the
+    default) traces them by increasing impact parameter hypot(alpha, beta): an escaping ray's
+    step count falls as it passes farther from the hole. A tensor of per-ray costs -- the step
+    counts of an earlier map of the same rays, as a fit has them -- traces them by decreasing
+    cost; ``"given"`` keeps the input order. The results come back in the input order, and are
+    the same bit for bit in every order."""
     import torch
 
     L = _bind()
@@ -101,6 +111,9 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
     a = alpha.to(dev, torch.float64).contiguous()
     b = beta.to(dev, torch.float64).contiguous()
     n = a.numel()
+    perm = _trace_order(order, a, b)
+    if perm is not None:
+        a, b = a[perm].contiguous(), b[perm].contiguous()
     p = _params(spin, inclination_deg, r_o, mass, integ, term, checkpoint_every, tape_capacity)
     if workspace is not None:
         need = int(L.krr_lensing_workspace_size(n, p.tape_capacity, p.checkpoint_every))
@@ -121,7 +134,34 @@ def lensing_map(alpha, beta, spin: float, inclination_deg: float, *, r_o: float 
                                      phi.data_ptr(), jac.data_ptr(), state.data_ptr(), steps.data_ptr(),
                                      status.data_ptr(), ws.data_ptr(), ws.numel(), stream))
     jac[:, :, 3] *= DEG  # per degree of inclination
-    return LensingResult(theta, phi, jac, state, steps, status, ws, p)
+    if perm is not None:
+        theta, phi, jac, state, steps, status = (_unpermute(x, perm) for x in (theta, phi, jac, state, steps, status))
+    return LensingResult(theta, phi, jac, state, steps, status, ws, p, perm)
+
+
+def _trace_order(order, alpha, beta):
+    """The permutation (input indices in trace order) that ``order`` asks for, or None."""
+    import torch
+
+    if isinstance(order, str):
+        if order == "given":
+            return None
+        if order == "impact":
+            return torch.argsort(torch.hypot(alpha, beta), stable=True)
+        raise ValueError(f"order must be 'impact', 'given' or a tensor of per-ray costs, got {order!r}")
+    cost = torch.as_tensor(order, device=alpha.device)
+    if cost.shape != alpha.shape:
+        raise ValueError(f"order: one cost per ray expected, shape {tuple(alpha.shape)}, got {tuple(cost.shape)}")
+    return torch.argsort(cost.to(torch.float64), descending=True, stable=True)
+
+
+def _unpermute(x, perm):
+    """Rows of ``x`` (in trace order) back in input order."""
+    import torch
+
+    out = torch.empty_like(x)
+    out[perm] = x
+    return out
 
 
 def workspace_bytes(n: int, *, checkpoint_every: int = 32, tape_capacity: int = 8192,
@@ -164,13 +204,19 @@ def replay(res: LensingResult, alpha, beta, spin: float, inclination_deg: float,
     a = alpha.to(dev, torch.float64).contiguous()
     b = beta.to(dev, torch.float64).contiguous()
     n = a.numel()
+    state, steps = res.state, res.n_steps
+    if res.perm is not None:  # the tape holds the rays in their trace order
+        a, b = a[res.perm].contiguous(), b[res.perm].contiguous()
+        state, steps = state[res.perm].contiguous(), steps[res.perm].contiguous()
     theta = torch.empty(n, dtype=torch.float64, device=dev)
     phi = torch.empty_like(theta)
     status = torch.empty(n, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(device).cuda_stream
-    _lib.check(L.krr_lensing_replay(device, ctypes.byref(p), a.data_ptr(), b.data_ptr(), n, res.state.data_ptr(),
-                                    res.n_steps.data_ptr(), theta.data_ptr(), phi.data_ptr(), status.data_ptr(),
+    _lib.check(L.krr_lensing_replay(device, ctypes.byref(p), a.data_ptr(), b.data_ptr(), n, state.data_ptr(),
+                                    steps.data_ptr(), theta.data_ptr(), phi.data_ptr(), status.data_ptr(),
                                     res.workspace.data_ptr(), res.workspace.numel(), stream))
+    if res.perm is not None:
+        theta, phi = _unpermute(theta, res.perm), _unpermute(phi, res.perm)
     return theta, phi
 
 
@@ -238,10 +284,14 @@ def fit_spin_inclination(alpha, beta, target_theta, target_phi, *, p0=(0.5, 50.0
     # One tape for every evaluation: the fit reads each result's map and Jacobian, never its tape.
     ws = torch.empty(workspace_bytes(alpha.numel()), dtype=torch.uint8, device=torch.device("cuda", device))
 
+    hint = "impact"  # then each evaluation's step counts order the next one's rays
+
     def evaluate(q):
-        nonlocal evaluations
+        nonlocal evaluations, hint
         evaluations += 1
-        res = lensing_map(alpha, beta, float(q[0]), float(q[1]), r_o=r_o, integ=integ, workspace=ws, device=device)
+        res = lensing_map(alpha, beta, float(q[0]), float(q[1]), r_o=r_o, integ=integ, workspace=ws, order=hint,
+                          device=device)
+        hint = res.n_steps
         ok = (res.status == 0) & (res.state == 1) & targets_ok
         d_th = res.theta - target_theta
         d_ph = torch.remainder(res.phi - target_phi + math.pi, 2.0 * math.pi) - math.pi

@@ -7,6 +7,7 @@ with ``fastmath=False``), so that each product and sum rounds separately.
 
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -23,7 +24,7 @@ def build(force: bool = False) -> Path:
     """Compile the oracle library if it is missing or older than its source; return its path."""
     if not force and LIB.exists() and LIB.stat().st_mtime >= SRC.stat().st_mtime:
         return LIB
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = LIB.with_suffix(f".so.{os.getpid()}.tmp")  # per process: concurrent builds must not share it
     cmd = ["g++", *FLAGS, str(SRC), "-o", str(tmp)]
     subprocess.run(cmd, check=True)
     tmp.replace(LIB)
