@@ -1091,6 +1091,17 @@ def lensing_line(K, args) -> dict:
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
     kernel_ms = shard.max_over_ranks(statistics.mean(ms))
+    # The same map with the rays ordered by the previous map's step counts, as the fit runs it.
+    ms_hint = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        K.lensing_map(alpha, beta, spin, incl, workspace=ws, order=res.n_steps, device=local)
+        e1.record(stream)
+        e1.synchronize()
+        ms_hint.append(e0.elapsed_time(e1))
+    res = K.lensing_map(alpha, beta, spin, incl, workspace=ws, device=local)  # the tape of the default order
     ok = int(((res.status == 0) & (res.state == 1)).sum().item())
     tape = A.tape_usage(res, device=local)
     steps = res.n_steps.double()
@@ -1153,6 +1164,9 @@ def lensing_line(K, args) -> dict:
                   "kernel": ("k_lensing_forward (one ray per thread) + k_lensing_reverse_staged (two threads per "
                              "ray, from the stage records) + k_lensing_reverse (checkpoint recomputation, for rays "
                              "the stage pool could not hold)"),
+                  "ray_order": ("increasing impact parameter hypot(alpha, beta), the default; by the previous "
+                                "map's step counts (as the fit runs it): "
+                                f"{shard.max_over_ranks(statistics.mean(ms_hint)):.3f} ms per map"),
                   "stage_tape": {"rays_from_records": tape["staged_rays"], "chunks_used": tape["chunks_used"],
                                  "chunks_held": tape["chunks_total"], "bytes_per_step": 240},
                   "l2": ("tape in HBM (one workspace for every call), written once by the forward pass and read "
