@@ -655,7 +655,8 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
       // Escaping photons near the shadow edge (krr_radial.cuh:near_band) pass near the
       // unstable photon orbit, which magnifies the FP32 stages' round-off in their exit
       // direction: they are traced in fast FP64 by a third kernel, and the mixed trace skips
-      // them.  It is launched first, one block filling each of a fifth of the SMs, and lets the
+      // them.  It is launched first, one block filling each of a third of the SMs (a fifth, a
+      // quarter and two fifths ran 3-7 % slower at 1024^2, the same at 2048^2), and lets the
       // critical kernel launch as soon as its blocks run; the critical kernel, launched as its
       // programmatic dependent, waits for it at its own exit, so the mixed trace's exit wait
       // covers all three.  Its blocks exit when its short queue is drained, and the mixed
@@ -666,7 +667,7 @@ int prepare_pipeline(int device, const krr_image* images, int n_images, long lon
       p.near_v = nv;
       p.nearby = p.crit;
       p.nearby.q = p.w.q4;
-      p.nearby.grid = std::max(1, std::min(sms - crit_sms - 1, sms / 5));
+      p.nearby.grid = std::max(1, std::min(sms - crit_sms - 1, sms / 3));
       p.nearby.block = nv->block;
       p.nearby.index = p.w.near_list;
       p.nearby.d_total = &p.w.q4->flagged;
