@@ -47,6 +47,13 @@ FLOP_PER_ACCEPT = 28
 FLOP_PER_RAY = 127
 
 
+
+def ordinal(k: int) -> str:
+    """1st, 2nd, 3rd, 4th, ..., 11th, 12th, 13th, 21st, ..."""
+    k = int(k)
+    suffix = "th" if 10 <= k % 100 <= 20 else {1: "st", 2: "nd", 3: "rd"}.get(k % 10, "th")
+    return f"{k}{suffix}"
+
 def algorithmic_flops(stats: dict) -> float:
     return FLOP_PER_ATTEMPT * stats["attempts"] + FLOP_PER_ACCEPT * stats["accepted"] + FLOP_PER_RAY * stats["photons"]
 
@@ -230,7 +237,7 @@ def cpu_baseline(specs, target_s: float = 15.0, keep: bool = False):
     stride = calibrate_stride(specs, target_s)
     n, dt, threads, kept = time_cpu_sample(specs, stride, 1, keep=True)
     line = {"value": n / dt, "unit": "rays/s", "cores": threads, "kind": "port",
-            "sample": f"every {stride}th photon of the {len(specs)}-image job ({n} rays, {dt:.1f} s), C++ oracle, "
+            "sample": f"every {ordinal(stride)} photon of the {len(specs)}-image job ({n} rays, {dt:.1f} s), C++ oracle, "
                       f"OpenMP {threads} threads"}
     return (line, kept) if keep else line
 
@@ -359,10 +366,10 @@ def run_reference(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "photons": total, "sample_stride": stride,
                    "photons_per_step": rays // max(args.steps, 1),
-                   "step": f"every {stride}th photon of the sweep (offset = step index), the same rays/s metric",
+                   "step": f"every {ordinal(stride)} photon of the sweep (offset = step index), the same rays/s metric",
                    "full_sweep_s_extrapolated": total / value},
         "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads, "kind": "port",
-                         "sample": f"every {stride}th photon per step ({rays // max(args.steps, 1)} rays/step), "
+                         "sample": f"every {ordinal(stride)} photon per step ({rays // max(args.steps, 1)} rays/step), "
                                    f"C++ restatement of the reference kernel, OpenMP {threads} threads"},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -837,7 +844,7 @@ def bisect_cpu_baseline(K, cases, target_s: float = 15.0) -> dict:
         n += n_k
         dt += dt_k
     return {"value": n / dt, "unit": "rays/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": (f"{n} first-halving rays (every {stride}th angle of each of the {len(cases)} cases, "
+            "sample": (f"{n} first-halving rays (every {ordinal(stride)} angle of each of the {len(cases)} cases, "
                        f"{reps} pass(es)), {dt:.1f} s")}
 
 
@@ -1043,7 +1050,7 @@ def lensing_cpu_baseline(K, a_np: np.ndarray, b_np: np.ndarray, spin: float, inc
             dirs.append(surface_directions(K, (K.Spacetime(1.0, s_), r_o), o["Y"], o["state"]))
         fd[:, :, p_] = (dirs[0] - dirs[1]) / (2 * h)
     line = {"value": idx.size / dt, "unit": "rays/s", "cores": threads, "kind": "port",
-            "sample": ((f"every {stride}th of the {a_np.size} rays" if stride > 1 else f"all {a_np.size} rays") +
+            "sample": ((f"every {ordinal(stride)} of the {a_np.size} rays" if stride > 1 else f"all {a_np.size} rays") +
                        f" ({idx.size} rays, {dt:.1f} s): central differences "
                        f"(h = 1e-6) of the oracle's integration, 8 traces per ray at rtol 1e-10, OpenMP {threads} "
                        f"threads")}
@@ -1159,7 +1166,7 @@ def lensing_line(K, args) -> dict:
                                    "seconds": fit_s}
     return _line("lensing-map adjoint rays/s per B200 (forward with tape + reverse sweep, 4 parameters)",
                  n_job / (kernel_ms * 1e-3), "rays/s", args, kernel_ms,
-                 {"workload": WORKLOADS["lensing"] + (f" (every {stride}th ray)" if stride > 1 else ""),
+                 {"workload": WORKLOADS["lensing"] + (f" (every {ordinal(stride)} ray)" if stride > 1 else ""),
                   "rays": n_job, "rays_per_gpu": n, "checkpoint_every": 32,
                   "kernel": ("k_lensing_forward (one ray per thread) + k_lensing_reverse_staged (two threads per "
                              "ray, from the stage records) + k_lensing_reverse (checkpoint recomputation, for rays "
