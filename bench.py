@@ -47,7 +47,6 @@ FLOP_PER_ACCEPT = 28
 FLOP_PER_RAY = 127
 
 
-
 def ordinal(k: int) -> str:
     """1st, 2nd, 3rd, 4th, ..., 11th, 12th, 13th, 21st, ..."""
     k = int(k)
