@@ -204,3 +204,28 @@ def test_lensing_workspace_sizes() -> None:
         assert extra == (-(-steps // 16) + n) * chunk, steps
     assert L.krr_lensing_workspace_size_staged(n, cap, k, -1) == 0
     assert L.krr_lensing_workspace_size_staged(-1, cap, k, 10) == 0
+
+
+def test_lensing_trace_order_permutations() -> None:
+    """The orders the lensing map can trace its rays in (host logic, no device): by increasing
+    impact parameter, by decreasing per-ray cost, or as given; un-permuting restores the rows."""
+    torch = pytest.importorskip("torch")
+    from kerrray_b200 import adjoint as A
+
+    alpha = torch.tensor([3.0, -0.5, 2.0, 0.0, -4.0], dtype=torch.float64)
+    beta = torch.tensor([0.0, 0.5, -2.0, 1.0, 0.0], dtype=torch.float64)
+    assert A._trace_order("given", alpha, beta) is None
+    imp = A._trace_order("impact", alpha, beta)
+    assert imp.tolist() == [1, 3, 2, 0, 4]  # hypot 0.71, 1, 2.83, 3, 4
+    cost = torch.tensor([10, 300, 20, 300, 5])
+    by_cost = A._trace_order(cost, alpha, beta)
+    assert by_cost.tolist() == [1, 3, 2, 0, 4]  # decreasing cost, ties in input order
+    rows = torch.arange(5.0) * 10
+    traced = rows[by_cost]
+    assert torch.equal(A._unpermute(traced, by_cost), rows)
+    jac = torch.arange(40.0).reshape(5, 2, 4)
+    assert torch.equal(A._unpermute(jac[imp], imp), jac)
+    with pytest.raises(ValueError):
+        A._trace_order("sideways", alpha, beta)
+    with pytest.raises(ValueError):
+        A._trace_order(torch.ones(4), alpha, beta)
