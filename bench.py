@@ -523,7 +523,7 @@ def mixed_vs_plain(K, local: int, stream, flush, name: str = "spin99_1024", orac
            "speedup_mixed_near_vs_plain": t["plain"] / t["near"],
            "mixed_near_mask_identical": bool(torch.equal(near.tensors["state"], ref)),
            "near_edge": int(ns["near_edge"]), "near_critical_ms": ns["critical_ms"],
-           "near_pipeline": "the same with the escaping photons within 0.3 M of the critical curve in fast FP64 "
+           "near_pipeline": "the same with the escaping photons within 0.35 M of the critical curve in fast FP64 "
                             "on SMs of their own (exit directions at the oracle's bar)",
            "mixed_kernel_only_rays_s": total / (t["bare"] * 1e-3),
            "mixed_kernel_roofline": {"achieved": mixed_tflops, "unit": "TFLOP/s", "fp32_peak": peak32,

@@ -70,7 +70,7 @@ enum {
                                within 1 % of its affine or step budget) in reference order: the
                                plain FP64 kernel's mask */
   KRR_RETRACE_CRITICAL_NEAR = 3  /* KRR_RETRACE_CRITICAL and, for a mixed trace, the escaping photons
-                               within 0.3 M of the critical curve traced in fast FP64 on SMs of their
+                               within 0.35 M of the critical curve traced in fast FP64 on SMs of their
                                own as well: exit directions within the oracle's bar there too */
 };
 

@@ -137,7 +137,7 @@ class LaunchConfig:
     # kernel: 0 off; 1 (RETRACE_EDGE) afterwards, every pixel not ESCAPED or CAPTURED or unlike a
     # neighbour; 2 (RETRACE_CRITICAL) the photons near the critical curve (analytic classes from
     # the radial potential) beside the main trace, then every photon unlike its class;
-    # 3 (RETRACE_CRITICAL_NEAR) that and, for a mixed trace, the escaping photons within 0.3 M of
+    # 3 (RETRACE_CRITICAL_NEAR) that and, for a mixed trace, the escaping photons within 0.35 M of
     # the critical curve in fast FP64 (their exit directions then meet the oracle's bar too).
     retrace: int = 0
     critical_sms: int = 0     # RETRACE_CRITICAL: SMs of the reference-order kernel (0: library default)
