@@ -298,7 +298,9 @@ KRR_API int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_c
  * accepted steps in all (their sum over the rays, plus one chunk of rounding per ray).  The rays
  * in flight take chunks first come, first served, so a pool well short of the total keeps
  * whole record sets only for the rays that finish before it runs out.
- * status[k]: 0 ok, 1 more accepted steps than tape_capacity, 2 neither ESCAPED nor CAPTURED. */
+ * status[k]: 0 ok, 1 more accepted steps than tape_capacity, 2 neither ESCAPED nor CAPTURED; a ray
+ * with status 1 or 2 gets NaN for theta, phi and its Jacobian, and krr_lensing_replay gives it NaN
+ * and the same status. */
 typedef struct krr_lens_params {
   double mass, spin;
   double radius, inclination_deg, phi_deg;

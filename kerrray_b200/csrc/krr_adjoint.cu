@@ -511,11 +511,12 @@ __global__ void __launch_bounds__(FWD_BLOCK, 3) k_lensing_forward(LensArgs A) {
     if (staged) record_copy(chunk + ((N - 1) % STAGE_CHUNK) * STEP_REC, ry.sh.slot);
   }
   record_wait_all();
-  // 3. the output at the termination surface (event-time correction)
+  // 3. the output at the termination surface (event-time correction); a ray whose tape ran
+  // out, or that reached neither surface, has no output (NaN, like its Jacobian)
   const double dr = ry.y[CR] - rs;
   const double fr = ry.f[CR];
-  A.theta[ray] = ry.y[CTH] - ry.f[CTH] / fr * dr;
-  A.phi[ray] = ry.y[CPH] - ry.f[CPH] / fr * dr;
+  A.theta[ray] = status == 0 ? ry.y[CTH] - ry.f[CTH] / fr * dr : CUDART_NAN;
+  A.phi[ray] = status == 0 ? ry.y[CPH] - ry.f[CPH] / fr * dr : CUDART_NAN;
   A.status[ray] = status;
   A.staged[ray] = (status == 0 && staged && N > 0) ? 1 : 0;
   double* rec = A.final_rec + ray * FINAL_REC;
@@ -794,10 +795,20 @@ __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(
 
 
 // Replay: the same camera and the recorded step sequence without the controller (the map the
-// adjoint differentiates), for finite-difference checks.
+// adjoint differentiates), for finite-difference checks.  A ray with more steps than the tape
+// holds (status 1) or that reached neither surface (status 2) has no recorded map: NaN.
 __global__ void __launch_bounds__(128) k_lensing_replay(LensArgs A) {
   const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n) return;
+  const long long n_rec = A.n_steps[ray];
+  const int st = (int)A.state[ray];
+  const int bad = (n_rec < 0 || n_rec > A.cap) ? 1 : (st != ESCAPED && st != CAPTURED) ? 2 : 0;
+  if (bad) {
+    A.theta[ray] = CUDART_NAN;
+    A.phi[ray] = CUDART_NAN;
+    A.status[ray] = bad;
+    return;
+  }
   const Params& P = A.P;
   double y0[8];
   camera_state_t<double>(A.alpha[ray], A.beta[ray], A.P.a, A.th_o, A.r_o, A.ph_o, A.mass, y0);

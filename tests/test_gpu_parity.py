@@ -773,6 +773,31 @@ def test_adjoint_results_do_not_depend_on_the_trace_order() -> None:
         A.lensing_map(alpha, beta, spin, incl, order="sideways")
 
 
+def test_adjoint_rays_beyond_the_tape_get_no_result() -> None:
+    """With a tape shorter than some rays' step counts: those rays report status 1 and NaN
+    (map, Jacobian, and replay through the tape); every other ray's results equal those of a
+    tape long enough for all, bit for bit."""
+    from kerrray_b200 import adjoint as A
+
+    alpha, beta = _lens_rays()
+    spin, incl = 0.8, 60.0
+    full = A.lensing_map(alpha, beta, spin, incl)
+    cap = int(full.n_steps.double().median().item())
+    short = A.lensing_map(alpha, beta, spin, incl, tape_capacity=cap)
+    over = (full.n_steps > cap).cpu().numpy()
+    assert 0 < over.sum() < over.size
+    status = short.status.cpu().numpy()
+    assert np.all(status[over] == 1) and np.all(status[~over] == 0)
+    for name in ("theta", "phi", "jac"):
+        a, b = getattr(short, name).cpu().numpy(), getattr(full, name).cpu().numpy()
+        assert np.all(np.isnan(a[over])), name
+        assert np.array_equal(a[~over], b[~over]), name
+    th, ph = A.replay(short, alpha, beta, spin, incl)
+    th, ph = th.cpu().numpy(), ph.cpu().numpy()
+    assert np.all(np.isnan(th[over])) and np.all(np.isnan(ph[over]))
+    assert np.array_equal(th[~over], short.theta.cpu().numpy()[~over])
+
+
 def torch_equal(x, y) -> bool:
     return bool((x == y).all())
 
