@@ -283,7 +283,10 @@ KRR_API int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_c
 
 /* The lensing map of one observer, differentiated: for n image points (alpha, beta) the terminal
  * celestial direction (theta_e, phi_e) -- theta and phi located on the termination surface
- * (escape radius, or capture radius) from the last accepted state by one step along the flow --
+ * (escape radius, or capture radius) from the last accepted state by one step along the flow;
+ * on the capture surface r_+ + epsilon the Boyer-Lindquist coordinates are singular (phi grows
+ * like log(r - r_+), the derivatives like 1 / (r - r_+)), so the derivatives are meant for
+ * escaping rays --
  * and its Jacobian d(theta_e, phi_e)/d(alpha, beta, spin, theta_o [rad]) (jac: n x 2 x 4), by the
  * adjoint of the discretised Dormand-Prince 5(4) map over the recorded accepted steps with the
  * controller held fixed.  FP64.  No counterpart in the reference (its gradients are finite
