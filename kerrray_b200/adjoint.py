@@ -239,8 +239,8 @@ class LensingFunction:
 
             class _F(torch.autograd.Function):
                 @staticmethod
-                def forward(ctx, a, b, s, i):
-                    res = lensing_map(a.detach(), b.detach(), float(s), float(i), **ctx_kw)
+                def forward(ctx, a, b, s, i, options):
+                    res = lensing_map(a.detach(), b.detach(), float(s), float(i), **options)
                     ctx.save_for_backward(res.jac)
                     return res.theta, res.phi
 
@@ -248,15 +248,11 @@ class LensingFunction:
                 def backward(ctx, g_theta, g_phi):
                     (jac,) = ctx.saved_tensors
                     g = g_theta[:, None] * jac[:, 0, :] + g_phi[:, None] * jac[:, 1, :]
-                    return g[:, 0], g[:, 1], g[:, 2].sum().reshape(()), g[:, 3].sum().reshape(())
+                    return g[:, 0], g[:, 1], g[:, 2].sum().reshape(()), g[:, 3].sum().reshape(()), None
 
             cls._fn = _F
-        global ctx_kw
-        ctx_kw = kw
-        return cls._fn.apply(alpha, beta, spin, inclination_deg)
-
-
-ctx_kw: dict = {}
+        # lensing_map's keyword options go in as a plain (non-tensor) argument of this call
+        return cls._fn.apply(alpha, beta, spin, inclination_deg, dict(kw))
 
 
 def fit_spin_inclination(alpha, beta, target_theta, target_phi, *, p0=(0.5, 50.0), iterations: int = 20,

@@ -897,6 +897,18 @@ def test_autograd_function_and_gauss_newton_fit() -> None:
     loss = ((th - target.theta) ** 2 + (ph - target.phi) ** 2).sum()
     loss.backward()
     assert torch.isfinite(a.grad).all() and float(s.grad) != 0.0 and float(i.grad) != 0.0
+    # the gradients are the chain rule through the map's own Jacobian at that point
+    at = A.lensing_map(alpha, beta, 0.7, 55.0)
+    assert torch.equal(at.theta, th.detach()) and torch.equal(at.phi, ph.detach())
+    g_t, g_p = 2.0 * (at.theta - target.theta), 2.0 * (at.phi - target.phi)
+    want = g_t[:, None] * at.jac[:, 0, :] + g_p[:, None] * at.jac[:, 1, :]
+    assert torch.allclose(a.grad, want[:, 0], rtol=1e-12, atol=0.0)
+    assert torch.allclose(s.grad, want[:, 2].sum(), rtol=1e-12, atol=0.0)
+    assert torch.allclose(i.grad, want[:, 3].sum(), rtol=1e-12, atol=0.0)
+    # lensing_map's options pass through apply (here the trace order, which changes no bit)
+    th2, _ = A.LensingFunction.apply(alpha, beta, torch.tensor(0.7, dtype=torch.float64),
+                                     torch.tensor(55.0, dtype=torch.float64), order="given")
+    assert torch.equal(th2, at.theta)
     mag = A.magnification(target.jac)
     assert bool(torch.isfinite(mag).all()) and float(mag.min()) > 0
     fit = A.fit_spin_inclination(alpha, beta, target.theta, target.phi, p0=(0.5, 50.0), iterations=20)
