@@ -347,6 +347,35 @@ __device__ __forceinline__ void rhs_separated(T dlt, T r, T s, T c, T pr, T pth,
   f[CPTH] = (isig * c) * fused(v, fused(lis, is, mo.ae), -a2s * bs);
 }
 
+// rhs_separated<float, true>, the mixed mode's right-hand side, with its six numerators
+// multiplied by 1 / Sigma as three packed pairs in the pairing of the mixed stage sums:
+// out[0] = (f_r, f_theta), out[1] = (f_pr, f_ptheta), out[2] = (f_t, f_phi), f_t (and, far,
+// f_r) as deviations.  Every value is the same operation on the same operands as in
+// rhs_separated (f_ptheta = F * (1/Sigma * cos) as there), so the results are its results bit
+// for bit, in three packed multiplies where it takes six, and with 2 M r formed once.
+__device__ __forceinline__ void rhs_separated_pairs(float dlt, float r, float s, float c, float pr, float pth,
+                                                    const Motion<float>& mo, float a, float a2, float m,
+                                                    float2 out[3], bool far) {
+  const float r2a2 = fmaf(r, r, a2);
+  const float as = a * s;
+  const float a2s = a * as;
+  const float k = fmaf(r2a2, mo.e, -mo.al);
+  const float isig = rcp_fast(fmaf(-a2s, s, r2a2));
+  const float kd = k * rcp_fast(dlt);
+  const float is = (mo.l != 0.0f) ? rcp_fast(s) : 0.0f;
+  const float lis = mo.l * is;
+  const float v = fmaf(-mo.ae, s, lis);
+  const float rm = r - m;
+  const float pr2 = pr * pr;
+  const float bs = fmaf(v, v, fmaf(-k, kd, fmaf(dlt, pr2, pth * pth))) * isig;
+  const float tmr = (m + m) * r;
+  out[0] = __fmul2_rn(make_float2(pr * (far ? fmaf(a2s, s, -tmr) : dlt), pth), make_float2(isig, isig));
+  out[1] = __fmul2_rn(make_float2(fmaf(r, bs, -fmaf(rm, pr2, kd * fmaf(kd, rm, mo.m2e * r))),
+                                  fmaf(v, fmaf(lis, is, mo.ae), -a2s * bs)),
+                      make_float2(isig, isig * c));
+  out[2] = __fmul2_rn(make_float2(tmr * kd, fmaf(a, kd, fmaf(lis, is, -mo.ae))), make_float2(isig, isig));
+}
+
 // The FP32 sincos_shift on packed pairs (fma/mul.rn.f32x2, sm_100): the sine and cosine
 // polynomials and the two rotation products advance together, every value the same operation
 // on the same operands as in the scalar form.  (The right-hand side stays scalar: packing its
@@ -527,7 +556,14 @@ struct Mixed {
     sh.mo.set((float)pt, (float)pph, (float)P.a);
     tr = accept_trig(y[CTH], tr);
     accepted(P, y, sh, tr);
-    rhs_f(P, sh.rd.y, sh.rd.x, sh.s0, sh.c0, sh.pp.x, sh.pp.y, sh.mo, f, sh.far);
+    float2 o[3];
+    rhs_f(P, sh.rd.y, sh.rd.x, sh.s0, sh.c0, sh.pp.x, sh.pp.y, sh.mo, o, sh.far);
+    f[CR] = o[0].x;
+    f[CTH] = o[0].y;
+    f[CPR] = o[1].x;
+    f[CPTH] = o[1].y;
+    f[CT] = o[2].x;
+    f[CPH] = o[2].y;
   }
 
   // The right-hand side at the stage input shadow + h * acc, from the pairs (r, theta) and
@@ -555,21 +591,22 @@ struct Mixed {
       sincos_reduced((double)fmaf(sh.psgn, dth, sh.ep), s, c);
       c *= sh.psgn;
     }
-    float f[NV];
-    rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, f, sh.far);
-    if (dev_r) *dev_r = f[CR];
-    k[0] = make_float2(sh.far ? fmaf(h, acc[1].x, f[CR]) : f[CR], f[CTH]);
-    k[1] = make_float2(f[CPR], f[CPTH]);
-    k[2] = make_float2(f[CT], f[CPH]);
+    float2 o[3];
+    rhs_f(P, rd.y, rd.x, s, c, pp.x, pp.y, sh.mo, o, sh.far);
+    if (dev_r) *dev_r = o[0].x;
+    k[0] = make_float2(sh.far ? fmaf(h, acc[1].x, o[0].x) : o[0].x, o[0].y);
+    k[1] = o[1];
+    k[2] = o[2];
   }
 
   // The right-hand side in FP32 at (r - r_plus = d, r, sin, cos, p_r, p_theta), its t component
   // as the deviation dt/dlambda - E and, with far, its r component as dr/dlambda - p_r
   // (rhs_separated): every stage, the FSAL values and the stage sums of t (and of r, far from the
-  // hole) hold deviations, and the step adds h E to t (and h p_r to r) in FP64.
+  // hole) hold deviations, and the step adds h E to t (and h p_r to r) in FP64.  The result comes
+  // as the stage sums' pairs (rhs_separated_pairs): (r, theta), (p_r, p_theta), (t, phi).
   __device__ static void rhs_f(const Params& P, float d, float rf, float s, float c, float pr, float pth,
-                               const Motion<float>& mo, float f[NV], bool far) {
-    rhs_separated<float, true>(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, f, far);
+                               const Motion<float>& mo, float2 out[3], bool far) {
+    rhs_separated_pairs(d * (d + P.f_rpm), rf, s, c, pr, pth, mo, P.f_a, P.f_a2, P.f_mass, out, far);
   }
 };
 
