@@ -229,3 +229,35 @@ def test_lensing_trace_order_permutations() -> None:
         A._trace_order("sideways", alpha, beta)
     with pytest.raises(ValueError):
         A._trace_order(torch.ones(4), alpha, beta)
+
+
+def test_lensing_entry_points_validate_before_device_work() -> None:
+    """krr_lensing_adjoint and krr_lensing_tape_usage reject bad arguments with KRR_ERR_INVALID /
+    KRR_ERR_UNSUPPORTED before any device call (the buffer addresses below are never read)."""
+    from kerrray_b200 import adjoint as A
+
+    L = A._bind()  # the package's own argument types
+    n = 1000
+    p = A._params(0.8, 60.0, 1000.0, 1.0, None, None, 32, 4096)
+    need = L.krr_lensing_workspace_size(n, 4096, 32)
+    fake = [0x10000 * (k + 1) for k in range(6)]  # device addresses of the outputs, never dereferenced
+
+    def call(params, ws, ws_bytes, bufs=fake, a=0x100000, b=0x200000):
+        return L.krr_lensing_adjoint(0, ctypes.byref(params), a, b, n, *bufs, ws, ws_bytes, None)
+
+    assert call(p, 0x400000, need - 256) == _lib.KRR_ERR_INVALID        # workspace too small
+    assert call(p, 0x400008, need) == _lib.KRR_ERR_INVALID              # not 256-byte aligned
+    assert "256-byte aligned" in _lib.lib().krr_last_error().decode()
+    assert call(p, 0x400000, need, bufs=[0] + fake[1:]) == _lib.KRR_ERR_INVALID  # a NULL output
+    bad = A.KrrLensParams.from_buffer_copy(p)
+    bad.checkpoint_every = 0
+    assert call(bad, 0x400000, need) == _lib.KRR_ERR_INVALID
+    rk4 = A._params(0.8, 60.0, 1000.0, 1.0, K.IntegratorOptions(method="rk4"), None, 32, 4096)
+    assert call(rk4, 0x400000, need) == _lib.KRR_ERR_UNSUPPORTED
+    # the usage query: outputs required; no rays, no device work
+    out = [ctypes.c_int64() for _ in range(3)]
+    assert L.krr_lensing_tape_usage(ctypes.byref(p), n, 0x400000, need, None, None, None, None) == _lib.KRR_ERR_INVALID
+    empty = L.krr_lensing_workspace_size_staged(0, 4096, 32, 0)
+    assert L.krr_lensing_tape_usage(ctypes.byref(p), 0, 0x400000, empty + 3840 * 5, *[ctypes.byref(o) for o in out],
+                                    None) == _lib.KRR_OK
+    assert out[0].value == 0 and out[1].value == 0 and out[2].value == 5
