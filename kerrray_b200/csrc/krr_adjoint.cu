@@ -423,9 +423,6 @@ __device__ void land_on_surface(const Params& P, Ray<M>& ry, const double y_prev
   h_last = h;
 }
 
-// Forward pass: camera, the integration with the reference controller recording the tape (step
-// sizes, checkpoints, stage records), the landing on the termination surface, the map's value,
-// and the landed final state.
 // The bulk copy of a record (shared -> global, 240 B, both 16 B aligned) and the waits on it.
 __device__ __forceinline__ void record_copy(double* dst, const double* src) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(src);
@@ -440,6 +437,9 @@ __device__ __forceinline__ void record_wait_all() { asm volatile("cp.async.bulk.
 
 constexpr int FWD_BLOCK = 128;
 
+// Forward pass: camera, the integration with the reference controller recording the tape (step
+// sizes, checkpoints, stage records), the landing on the termination surface, the map's value,
+// and the landed final state.
 __global__ void __launch_bounds__(FWD_BLOCK, 3) k_lensing_forward(LensArgs A) {
   __shared__ __align__(16) double recs[FWD_BLOCK * STEP_REC];
   const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
