@@ -439,8 +439,10 @@ constexpr int FWD_BLOCK = 128;
 
 // Forward pass: camera, the integration with the reference controller recording the tape (step
 // sizes, checkpoints, stage records), the landing on the termination surface, the map's value,
-// and the landed final state.
-__global__ void __launch_bounds__(FWD_BLOCK, 3) k_lensing_forward(LensArgs A) {
+// and the landed final state.  Two blocks per SM (228 registers, no spills): a map of more rays
+// than that holds starts its later blocks as earlier ones end, the rays in trace order (longest
+// first by default); three blocks per SM (168 registers, spilling) ran 0.5-1 % slower.
+__global__ void __launch_bounds__(FWD_BLOCK, 2) k_lensing_forward(LensArgs A) {
   __shared__ __align__(16) double recs[FWD_BLOCK * STEP_REC];
   const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n) return;
