@@ -260,15 +260,11 @@ def surface_directions(K, spec, Y, state) -> np.ndarray:
 
 
 def direction_error(d1: np.ndarray, d2: np.ndarray) -> np.ndarray:
-    """The angle (rad) between the directions (theta, phi) of each row on the escape sphere:
-    2 asin(|u1 - u2| / 2) of their unit vectors, well conditioned for small angles. A ray leaving
-    close to a pole has an ill-conditioned phi (a displacement delta on the sky moves phi by
-    delta / sin theta), so the coordinate differences overstate its error there by 1 / sin theta."""
-    def unit(d):
-        s = np.sin(d[:, 0])
-        return np.stack([s * np.cos(d[:, 1]), s * np.sin(d[:, 1]), np.cos(d[:, 0])], axis=1)
+    """The angle (rad) between the directions (theta, phi) of each row on the escape sphere
+    (``kerrray_b200.direction_angle``)."""
+    from kerrray_b200 import direction_angle
 
-    return 2.0 * np.arcsin(np.minimum(1.0, 0.5 * np.linalg.norm(unit(d1) - unit(d2), axis=1)))
+    return direction_angle(d1[:, 0], d1[:, 1], d2[:, 0], d2[:, 1])
 
 
 def component_error(d1: np.ndarray, d2: np.ndarray) -> np.ndarray:

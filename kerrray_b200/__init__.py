@@ -47,6 +47,7 @@ from kerrray_b200.sweep import (
     LaunchConfig,
     SweepResult,
     analytic_classes,
+    direction_angle,
     escape_directions,
     trig_eval,
     order_by_cost,
@@ -84,6 +85,6 @@ __all__ = [
     "SweepResult", "TerminationOptions", "TerminationState", "autotune", "available_backends", "compute_shadow",
     "get_backend", "initial_states", "initial_states_at", "list_variants", "max_attempts", "order_by_cost",
     "outer_horizon", "register_with_kerrray", "shadow_mask_int8", "state_counts", "trace_images", "trace_rays",
-    "RETRACE_CRITICAL", "RETRACE_CRITICAL_NEAR", "RETRACE_EDGE", "analytic_classes", "escape_directions", "trig_eval",
+    "RETRACE_CRITICAL", "RETRACE_CRITICAL_NEAR", "RETRACE_EDGE", "analytic_classes", "direction_angle", "escape_directions", "trig_eval",
     "DiskImage", "DiskModel", "load_disk_image_arrays", "render_disk", "save_disk_image",
 ]

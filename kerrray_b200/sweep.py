@@ -53,6 +53,22 @@ def escape_directions(spacetime, Y, state, r_surface: float):
     return theta, phi
 
 
+def direction_angle(theta1, phi1, theta2, phi2) -> np.ndarray:
+    """The angle (rad) between the directions (theta1, phi1) and (theta2, phi2) on the escape
+    sphere, per ray: 2 asin(|u1 - u2| / 2) of their unit vectors, well conditioned for small
+    angles. Next to a pole phi alone is ill-conditioned (a displacement d on the sky moves phi by
+    d / sin theta), so this, not max(|d theta|, |d phi|), measures how far two integrations of a
+    ray landed apart. NaN where either direction is NaN (a ray not escaped)."""
+    t1, p1, t2, p2 = (np.asarray(x, dtype=np.float64) for x in (theta1, phi1, theta2, phi2))
+
+    def unit(t, p):
+        st = np.sin(t)
+        return np.stack([st * np.cos(p), st * np.sin(p), np.cos(t)], axis=-1)
+
+    chord = np.linalg.norm(unit(t1, p1) - unit(t2, p2), axis=-1)
+    return 2.0 * np.arcsin(np.minimum(1.0, 0.5 * chord))
+
+
 def trig_eval(which: int, theta, delta=None):
     """The step kernels' sine and cosine forms at the angles of the float64 CUDA tensor ``theta``
     (``krr_trig_eval``): 0 the FP32 sine/cosine of an FP64 angle (mixed accepted states), 1 the

@@ -282,13 +282,8 @@ def _spin99_specs(res: int):
 
 
 def _direction_error(d1: np.ndarray, d2: np.ndarray) -> np.ndarray:
-    """The angle (rad) between the directions (theta, phi) of each row on the escape sphere,
-    2 asin(|u1 - u2| / 2) of their unit vectors (phi alone is ill-conditioned next to a pole)."""
-    def unit(d):
-        s = np.sin(d[:, 0])
-        return np.stack([s * np.cos(d[:, 1]), s * np.sin(d[:, 1]), np.cos(d[:, 0])], axis=1)
-
-    return 2.0 * np.arcsin(np.minimum(1.0, 0.5 * np.linalg.norm(unit(d1) - unit(d2), axis=1)))
+    """The angle (rad) between the directions (theta, phi) of each row on the escape sphere."""
+    return K.direction_angle(d1[:, 0], d1[:, 1], d2[:, 0], d2[:, 1])
 
 
 def _surface_dirs(st, Y, state, r_esc: float) -> np.ndarray:

@@ -132,3 +132,21 @@ def test_winding_prediction_and_initial_states_match_reference() -> None:
         for j, delta in enumerate(d["deltas"]):
             y = V.equatorial_photon(st, 50.0, float(d["b_c"][k]) * (1 + float(delta)), prograde=bool(prograde))
             assert np.allclose(y, d["Y0"][k][j], rtol=1e-14, atol=0.0)
+
+
+def test_direction_angle_is_the_angle_on_the_sphere() -> None:
+    """direction_angle against the spherical law of cosines where that is well conditioned, the
+    small-angle form next to a pole (where phi alone overstates the distance by 1 / sin theta),
+    wrapping in phi, and NaN for a ray that did not escape."""
+    rng = np.random.default_rng(5)
+    t1, p1 = rng.uniform(0.2, 2.9, 500), rng.uniform(-np.pi, np.pi, 500)
+    t2, p2 = rng.uniform(0.2, 2.9, 500), rng.uniform(-np.pi, np.pi, 500)
+    cos_d = np.cos(t1) * np.cos(t2) + np.sin(t1) * np.sin(t2) * np.cos(p1 - p2)
+    ref = np.arccos(np.clip(cos_d, -1.0, 1.0))
+    big = ref > 1e-2  # the law of cosines loses digits for small angles
+    assert np.allclose(K.direction_angle(t1, p1, t2, p2)[big], ref[big], rtol=1e-12, atol=0)
+    th = np.pi - 0.012
+    d = K.direction_angle(th, 1.0, th, 1.0 + 1e-4)
+    assert abs(d - np.sin(th) * 1e-4) < 1e-12          # 1.2e-6 rad, not 1e-4
+    assert abs(K.direction_angle(1.0, np.pi - 1e-7, 1.0, -np.pi + 1e-7) - np.sin(1.0) * 2e-7) < 1e-15
+    assert np.isnan(K.direction_angle(np.nan, 0.0, 1.0, 0.0))
