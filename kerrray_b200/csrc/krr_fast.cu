@@ -242,8 +242,17 @@ cudaError_t count_nonfinite(const double* x, long long n, unsigned long long* co
   return cudaGetLastError();
 }
 
+// The fast64 bisection at three blocks per SM (168 registers, spilling 44 B) only for a study
+// large enough to keep those lanes at most 3/4 of its items (run_bisect's rule); below that at
+// two blocks per SM, whose register budget holds the whole kernel (188 registers, no spills:
+// 2.5 % faster on the 51,840-item edge study).
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s) {
-  return mixed ? run_bisect<Mixed, 128, 1>(a, s) : run_bisect<Fast64, 128, 3>(a, s);
+  if (mixed) return run_bisect<Mixed, 128, 1>(a, s);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (4LL * sms * 3 * 128 <= 3LL * a.n_items) return run_bisect<Fast64, 128, 3>(a, s);
+  return run_bisect<Fast64, 128, 2>(a, s);
 }
 
 }  // namespace krr
