@@ -1165,7 +1165,7 @@ def lensing_line(K, args) -> dict:
                   "rays": n_job, "rays_per_gpu": n, "checkpoint_every": 32,
                   "kernel": ("k_lensing_forward (one ray per thread) + k_lensing_reverse_staged (two threads per "
                              "ray, from the stage records) + k_lensing_reverse (checkpoint recomputation, for rays "
-                             "the stage pool could not hold)"),
+                             "the stage pool could not hold), for each half of the rays, the halves on two streams"),
                   "ray_order": ("increasing impact parameter hypot(alpha, beta), the default; by the previous "
                                 "map's step counts (as the fit runs it): "
                                 f"{shard.max_over_ranks(statistics.mean(ms_hint)):.3f} ms per map"),
@@ -1174,7 +1174,7 @@ def lensing_line(K, args) -> dict:
                   "l2": ("tape in HBM (one workspace for every call), written once by the forward pass and read "
                          "once by the reverse sweep: step sizes (n x 8192 x 8 B) and 240 B of stage records per "
                          "accepted step")},
-                 e2e=e2e, gpu_launches=3 * args.steps,
+                 e2e=e2e, gpu_launches=(6 if n > 256 else 3) * args.steps,  # 3 kernels per half of the rays
                  roofline=roofline, cpu_baseline=cpu, clocks=clocks.summary(),
                  rays_ok=ok, accepted_steps={"mean": float(steps.mean().item()), "max": int(steps.max().item()),
                                              "total": int(total_steps)},

@@ -303,7 +303,11 @@ KRR_API int krr_bisect_edges(int device, const krr_edge_case* cases, int32_t n_c
  * whole record sets only for the rays that finish before it runs out.
  * status[k]: 0 ok, 1 more accepted steps than tape_capacity, 2 neither ESCAPED nor CAPTURED; a ray
  * with status 1 or 2 gets NaN for theta, phi and its Jacobian, and krr_lensing_replay gives it NaN
- * and the same status. */
+ * and the same status.
+ * Asynchronous on `stream`: beyond 256 rays the second half of them runs on a stream of the
+ * library's own, forked from `stream` and joined back to it before the call returns, so work
+ * ordered after the call on `stream` sees every ray's results, and a capture of `stream` holds
+ * both halves. */
 typedef struct krr_lens_params {
   double mass, spin;
   double radius, inclination_deg, phi_deg;

@@ -205,6 +205,8 @@ struct Context {
   cudaEvent_t h2d_ev[4] = {};           // each chunk's Y0 on the device
   cudaStream_t trace2 = nullptr;        // every other chunk's trace, so consecutive traces overlap their tails
   cudaEvent_t fork_ev = nullptr;        // trace2 starts after the setup on the main stream
+  cudaStream_t lens_aux = nullptr;      // the lensing map's second half of the rays
+  cudaEvent_t lens_fork = nullptr, lens_join = nullptr;
   int sm_count = 0;
   DevBuf buf[B_COUNT];
 };
@@ -232,6 +234,9 @@ int get_context(int device, Context** out) {
     KRR_CUDA(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking));
     KRR_CUDA(cudaStreamCreateWithFlags(&c->trace2, cudaStreamNonBlocking));
     KRR_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    KRR_CUDA(cudaStreamCreateWithFlags(&c->lens_aux, cudaStreamNonBlocking));
+    KRR_CUDA(cudaEventCreateWithFlags(&c->lens_fork, cudaEventDisableTiming));
+    KRR_CUDA(cudaEventCreateWithFlags(&c->lens_join, cudaEventDisableTiming));
     for (auto& ev : c->chunk_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     for (auto& ev : c->h2d_ev) KRR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     KRR_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
@@ -1319,7 +1324,14 @@ int krr_lensing_adjoint(int device, const krr_lens_params* params, const double*
     return fail(KRR_ERR_INVALID, "device buffers must not be NULL");
   if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
     return fail(KRR_ERR_INVALID, "the workspace must be 256-byte aligned (as cudaMalloc returns it)");
+  Context* c = nullptr;
+  rc = get_context(device, &c);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
   KRR_CUDA(cudaSetDevice(device));
+  L.aux = c->lens_aux;
+  L.ev_fork = c->lens_fork;
+  L.ev_join = c->lens_join;
   L.alpha = d_alpha;
   L.beta = d_beta;
   L.theta = d_theta;

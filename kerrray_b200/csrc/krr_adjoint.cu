@@ -296,7 +296,7 @@ struct LensArgs {
   int cap;  // tape capacity (accepted steps per ray)
   const double* alpha;
   const double* beta;
-  long long n;
+  long long first, n;  // this launch's rays: [first, n)
   double* theta;
   double* phi;
   double* jac;  // (n, 2, 4): rows theta_e, phi_e; columns alpha, beta, spin, theta_o (rad)
@@ -444,7 +444,7 @@ constexpr int FWD_BLOCK = 128;
 // first by default); three blocks per SM (168 registers, spilling) ran 0.5-1 % slower.
 __global__ void __launch_bounds__(FWD_BLOCK, 2) k_lensing_forward(LensArgs A) {
   __shared__ __align__(16) double recs[FWD_BLOCK * STEP_REC];
-  const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ray = A.first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n) return;
   const Params& P = A.P;
   double y0[8];
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(FWD_BLOCK, 2) k_lensing_forward(LensArgs A) {
 // k_lensing_reverse.
 __global__ void __launch_bounds__(128) k_lensing_reverse_staged(LensArgs A) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long ray = t >> 1;
+  const long long ray = A.first + (t >> 1);
   const int row = (int)(t & 1);  // 0: theta_e, 1: phi_e
   if (ray >= A.n || !A.staged[ray]) return;
   const Params& P = A.P;
@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(128) k_lensing_reverse_staged(LensArgs A) {
 #define KRR_LENS_REVERSE_MINB 1  // resident blocks per SM the reverse kernel's registers allow for
 #endif
 __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(LensArgs A) {
-  const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ray = A.first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n || A.staged[ray]) return;
   double* J = A.jac + ray * 8;
   if (A.status[ray] != 0) {
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(128, KRR_LENS_REVERSE_MINB) k_lensing_reverse(
 // adjoint differentiates), for finite-difference checks.  A ray with more steps than the tape
 // holds (status 1) or that reached neither surface (status 2) has no recorded map: NaN.
 __global__ void __launch_bounds__(128) k_lensing_replay(LensArgs A) {
-  const long long ray = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long ray = A.first + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ray >= A.n) return;
   const long long n_rec = A.n_steps[ray];
   const int st = (int)A.state[ray];
@@ -866,12 +866,35 @@ cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s) {
   }
   cudaError_t e = cudaMemsetAsync(L.pool_next, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
-  k_lensing_forward<<<grid, block, 0, s>>>(A);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_lensing_reverse_staged<<<(unsigned)((2 * L.n + block - 1) / block), block, 0, s>>>(A);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_lensing_reverse<<<grid, block, 0, s>>>(A);
-  return cudaGetLastError();
+  // Two halves (the first rounded to whole blocks) on two streams when the caller gave a second:
+  // the half whose forward pass ends first runs its reverse sweeps beside the other's forward
+  // tail (5.5 against 5.8 ms for the 55k-ray edge map; halves of 35, 42 and 58 % of the rays no
+  // faster, four quarters, whose forward passes fill too few SMs, 7.0 ms).  The halves share the
+  // stage pool, first come first served; every ray's results are the same either way.
+  const bool split = L.aux && L.n > 2 * block;
+  const long long half = split ? (L.n / 2 + block - 1) / block * block : L.n;
+  if (split) {
+    if ((e = cudaEventRecord(L.ev_fork, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(L.aux, L.ev_fork, 0)) != cudaSuccess) return e;
+  }
+  for (int part = 0; part < (split ? 2 : 1); ++part) {
+    cudaStream_t st = part ? L.aux : s;
+    A.first = part ? half : 0;
+    A.n = part ? L.n : half;
+    const long long cnt = A.n - A.first;
+    const unsigned g = (unsigned)((cnt + block - 1) / block);
+    k_lensing_forward<<<g, block, 0, st>>>(A);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_lensing_reverse_staged<<<(unsigned)((2 * cnt + block - 1) / block), block, 0, st>>>(A);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_lensing_reverse<<<g, block, 0, st>>>(A);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (split) {
+    if ((e = cudaEventRecord(L.ev_join, L.aux)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, L.ev_join, 0)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace krr

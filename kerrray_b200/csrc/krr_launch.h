@@ -69,6 +69,11 @@ struct LensLaunch {
   unsigned long long* pool_next;  // chunks handed out (zeroed before the forward kernel)
   int* chunk_tab;                 // (n, cap / STAGE_CHUNK + 1)
   unsigned char* staged;          // (n): the ray's whole stage tape is in the pool
+  // A second stream and two events of the caller's: with them the rays run as two halves, the
+  // second on `aux` (forked from and joined back to the launch stream), so that one half's
+  // reverse sweep fills the SMs the other half's forward pass leaves idle.  Null: one stream.
+  cudaStream_t aux;
+  cudaEvent_t ev_fork, ev_join;
 };
 cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s);
 

@@ -770,6 +770,31 @@ def test_adjoint_results_do_not_depend_on_the_trace_order() -> None:
         A.lensing_map(alpha, beta, spin, incl, order="sideways")
 
 
+def test_adjoint_halves_on_two_streams_are_each_rays_own_map() -> None:
+    """Beyond 256 rays the map runs as two halves, the second on a stream of the library's own:
+    launched on a side stream, the results read on that stream right after the call equal, bit
+    for bit, those of maps of 200 rays at a time (one stream each)."""
+    import torch
+    from kerrray_b200 import adjoint as A
+
+    alpha, beta = _lens_rays(n_side=32)
+    n = alpha.numel()
+    assert n > 256
+    spin, incl = 0.8, 60.0
+    names = ("theta", "phi", "jac", "state", "n_steps", "status")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        res = A.lensing_map(alpha, beta, spin, incl, order="given")
+        snap = {name: getattr(res, name).clone() for name in names}
+    side.synchronize()
+    for lo in range(0, n, 200):
+        part = A.lensing_map(alpha[lo:lo + 200], beta[lo:lo + 200], spin, incl, order="given")
+        for name in names:
+            assert torch_equal(snap[name][lo:lo + 200], getattr(part, name)), (lo, name)
+    th, ph = A.replay(res, alpha, beta, spin, incl)
+    assert torch_equal(th, res.theta) and torch_equal(ph, res.phi)
+
+
 def test_adjoint_rays_beyond_the_tape_get_no_result() -> None:
     """With a tape shorter than some rays' step counts: those rays report status 1 and NaN
     (map, Jacobian, and replay through the tape); every other ray's results equal those of a
