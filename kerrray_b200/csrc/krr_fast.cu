@@ -244,7 +244,7 @@ cudaError_t count_nonfinite(const double* x, long long n, unsigned long long* co
 
 // The fast64 bisection at three blocks per SM (168 registers, spilling 44 B) only for a study
 // large enough to keep those lanes at most 3/4 of its items (run_bisect's rule); below that at
-// two blocks per SM, whose register budget holds the whole kernel (188 registers, no spills:
+// two blocks per SM, whose register budget holds the whole kernel (186-188 registers, no spills:
 // 2.5 % faster on the 51,840-item edge study).
 cudaError_t fast_bisect(bool mixed, const EdgeArgs& a, cudaStream_t s) {
   if (mixed) return run_bisect<Mixed, 128, 1>(a, s);
