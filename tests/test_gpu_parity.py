@@ -793,6 +793,10 @@ def test_adjoint_halves_on_two_streams_are_each_rays_own_map() -> None:
             assert torch_equal(snap[name][lo:lo + 200], getattr(part, name)), (lo, name)
     th, ph = A.replay(res, alpha, beta, spin, incl)
     assert torch_equal(th, res.theta) and torch_equal(ph, res.phi)
+    # 257 rays: halves of 128 and 129 rays
+    edge = A.lensing_map(alpha[:257], beta[:257], spin, incl, order="given")
+    for name in names:
+        assert torch_equal(getattr(edge, name), snap[name][:257]), name
 
 
 def test_adjoint_rays_beyond_the_tape_get_no_result() -> None:
