@@ -877,24 +877,27 @@ cudaError_t lensing_adjoint(const LensLaunch& L, bool replay, cudaStream_t s) {
     if ((e = cudaEventRecord(L.ev_fork, s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(L.aux, L.ev_fork, 0)) != cudaSuccess) return e;
   }
-  for (int part = 0; part < (split ? 2 : 1); ++part) {
+  for (int part = 0; part < (split ? 2 : 1) && e == cudaSuccess; ++part) {
     cudaStream_t st = part ? L.aux : s;
     A.first = part ? half : 0;
     A.n = part ? L.n : half;
     const long long cnt = A.n - A.first;
     const unsigned g = (unsigned)((cnt + block - 1) / block);
     k_lensing_forward<<<g, block, 0, st>>>(A);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
     k_lensing_reverse_staged<<<(unsigned)((2 * cnt + block - 1) / block), block, 0, st>>>(A);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
     k_lensing_reverse<<<g, block, 0, st>>>(A);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = cudaGetLastError();
   }
+  // Once forked, the second stream joins back even after a failed launch, so that a capture of
+  // the caller's stream can still end; the first error is the one returned.
   if (split) {
-    if ((e = cudaEventRecord(L.ev_join, L.aux)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(s, L.ev_join, 0)) != cudaSuccess) return e;
+    cudaError_t j = cudaEventRecord(L.ev_join, L.aux);
+    if (j == cudaSuccess) j = cudaStreamWaitEvent(s, L.ev_join, 0);
+    if (e == cudaSuccess) e = j;
   }
-  return cudaSuccess;
+  return e;
 }
 
 }  // namespace krr
