@@ -254,6 +254,10 @@ def test_lensing_entry_points_validate_before_device_work() -> None:
     assert call(bad, 0x400000, need) == _lib.KRR_ERR_INVALID
     rk4 = A._params(0.8, 60.0, 1000.0, 1.0, K.IntegratorOptions(method="rk4"), None, 32, 4096)
     assert call(rk4, 0x400000, need) == _lib.KRR_ERR_UNSUPPORTED
+    import torch
+
+    if not torch.cuda.is_available():  # valid arguments reach the device check and stop there
+        assert call(p, 0x400000, need) == _lib.KRR_ERR_NO_DEVICE
     # the usage query: outputs required; no rays, no device work
     out = [ctypes.c_int64() for _ in range(3)]
     assert L.krr_lensing_tape_usage(ctypes.byref(p), n, 0x400000, need, None, None, None, None) == _lib.KRR_ERR_INVALID
