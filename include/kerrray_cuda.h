@@ -5,7 +5,8 @@
  * registry.  Every entry point takes plain pointers and sizes; none keeps a pointer after it
  * returns.  All functions return a status code (KRR_OK on success); krr_last_error() gives a
  * thread-local message for the last failure on the calling thread.  Calls are thread-safe: the
- * host-buffer entry points serialise per device.
+ * host-buffer entry points serialise per device, and krr_lensing_adjoint holds the same lock
+ * while it enqueues its work (on the caller's stream and the library's second stream).
  *
  * Reference interfaces replaced (file:line within joelprince2601/kerrray):
  *   krr_integrate_batch         Backend.integrate_batch
