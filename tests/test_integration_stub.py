@@ -1,0 +1,56 @@
+"""The ctypes stub that INTEGRATION.md gives a KerrRay maintainer: its structures have the ABI's
+layout (the package's own bindings of include/kerrray_cuda.h), and on a host without a device
+its constructor raises BackendUnavailable, as KerrRay's registry expects (base.py:71-82)."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from kerrray_b200 import _lib
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _stub_source() -> str:
+    text = (ROOT / "INTEGRATION.md").read_text()
+    blocks = re.findall(r"```python\n(.*?)```", text, flags=re.S)
+    src = [b for b in blocks if "class CudaBackend" in b]
+    assert len(src) == 1
+    return src[0]
+
+
+def _layout(struct) -> list[tuple[str, int, int]]:
+    return [(name, getattr(struct, name).offset, getattr(struct, name).size) for name, _ in struct._fields_]
+
+
+class BackendUnavailable(RuntimeError):
+    """Stands in for kerrray.raytracing.backends.base.BackendUnavailable."""
+
+
+def _exec_stub() -> dict:
+    ns = {"BackendUnavailable": BackendUnavailable, "BatchResult": dict}
+    src = _stub_source().replace('"libkerrray_cuda.so"', repr(str(_lib.LIB_PATH)))
+    exec(compile(src, "INTEGRATION.md", "exec"), ns)
+    return ns
+
+
+def test_stub_structures_have_the_abi_layout() -> None:
+    ns = _exec_stub()
+    assert ctypes.sizeof(ns["_Opts"]) == ctypes.sizeof(_lib.KrrOptions)
+    assert _layout(ns["_Opts"]) == _layout(_lib.KrrOptions)
+    assert ctypes.sizeof(ns["_Res"]) == ctypes.sizeof(_lib.KrrResult)
+    assert _layout(ns["_Res"]) == _layout(_lib.KrrResult)
+
+
+def test_stub_without_a_device_raises_backend_unavailable() -> None:
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    if not _lib.LIB_PATH.exists():
+        pytest.skip("library not built")
+    ns = _exec_stub()
+    with pytest.raises(BackendUnavailable):
+        ns["CudaBackend"]()
