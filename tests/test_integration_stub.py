@@ -1,6 +1,7 @@
 """The ctypes stub that INTEGRATION.md gives a KerrRay maintainer: its structures have the ABI's
 layout (the package's own bindings of include/kerrray_cuda.h), and on a host without a device
-its constructor raises BackendUnavailable, as KerrRay's registry expects (base.py:71-82)."""
+its constructor raises BackendUnavailable, as KerrRay's registry expects (base.py:71-82); the C
+example compiles against the header."""
 from __future__ import annotations
 
 import ctypes
@@ -54,3 +55,25 @@ def test_stub_without_a_device_raises_backend_unavailable() -> None:
     ns = _exec_stub()
     with pytest.raises(BackendUnavailable):
         ns["CudaBackend"]()
+
+
+def test_c_example_compiles_against_the_header(tmp_path) -> None:
+    """The C example (the mixed-precision mask) inside a function that declares its inputs:
+    gcc accepts it against include/kerrray_cuda.h with every warning an error."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not found")
+    text = (ROOT / "INTEGRATION.md").read_text()
+    blocks = re.findall(r"```c\n(.*?)```", text, flags=re.S)
+    assert len(blocks) == 1
+    src = tmp_path / "example.c"
+    src.write_text('#include "kerrray_cuda.h"\n'
+                   "int example(const krr_image* images, int32_t n_images, int64_t total_photons, krr_result d_out,\n"
+                   "            void* d_ws, void* stream) {\n"
+                   "  krr_stats stats;\n" + blocks[0] + "  return (int)stats.critical;\n}\n")
+    p = subprocess.run([gcc, "-std=c11", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I", str(ROOT / "include"),
+                        str(src)], capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
