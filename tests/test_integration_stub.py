@@ -1,4 +1,4 @@
-"""The ctypes stub that INTEGRATION.md gives a KerrRay maintainer: its structures have the ABI's
+"""The ctypes stub that the integration guide gives a KerrRay maintainer: its structures have the ABI's
 layout (the package's own bindings of include/kerrray_cuda.h), and on a host without a device
 its constructor raises BackendUnavailable, as KerrRay's registry expects (base.py:71-82); the C
 example compiles against the header."""
